@@ -1,0 +1,374 @@
+"""Benchmark of the batched B+tree point search on B200.
+
+Workload (the headline): a 2^26-key tree at fanout 64 (keys uniform in
+[0, 2^63), value = splitmix64(key) >> 1), one batch of 2^24 point queries
+with 90% hits, seeded synthetic data.  A step is one batch through
+BPlusTree.search (pre-sort + search + results in query order).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Under torchrun each rank runs an independent
+replica of the tree on its own GPU with its own query batch (the path does
+not shard: replicas only); ``value`` is all ranks' queries over the slowest
+rank's device time.
+
+``--impl reference`` times the reference's own CPU B+tree
+(open-harmonia/src, compiled into oracle/_ref/libhmref.so) on the same keys
+and queries with all host threads: OpenMP over BPlusTree::search, the loop
+of search_cpu_test (open-harmonia/src/main.cpp:772-812).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mqueries/s on 2^26-key tree (1 B200) vs plain batch; serving p50/p99 latency"
+UNIT = "Mqueries/s"
+FALLBACK_PEAK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--keys-log2", type=int, default=26)
+    ap.add_argument("--queries-log2", type=int, default=24)
+    ap.add_argument("--hit", type=float, default=0.9)
+    ap.add_argument("--fanout", type=int, default=64)
+    ap.add_argument("--leaf-cap", type=int, default=16)
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (use the flags below)")
+    ap.add_argument("--group-width", type=int, default=4)
+    ap.add_argument("--qpg", type=int, default=2)
+    ap.add_argument("--sort-bits", type=int, default=-1)
+    ap.add_argument("--hints", type=int, default=1)
+    ap.add_argument("--cpu-sample-log2", type=int, default=22)
+    ap.add_argument("--extras", type=int, default=1, help="also time plain / pre-sorted input / e2e")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_PEAK_GBS, "fallback"
+
+
+def algorithmic_bytes_per_query(fanout: int) -> int:
+    """Bytes a point query must move at 2^26 keys: 8 B key in + 8 B value out,
+    the DRAM-resident level (the leaves: one 8-entry index + one 8-key slice,
+    64 B + 64 B, or the 128-B row of a 16-key leaf), and one 32-B value sector.
+    Inner levels are L2-resident.  Fanout 128 adds its 128-B index + 64-B
+    slice for the last inner level, which no longer fits L2."""
+    return 176 if fanout == 64 else 240
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+                self.lines = [l for l in out.splitlines() if l.strip()]
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    from harmonia_b200 import datagen as dg
+    from oracle import pyoracle as po
+
+    if not po.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhmref.so is not built"}))
+        return 0
+    n = 1 << args.keys_log2
+    keys = dg.gen_keys(n, 1)
+    vals = dg.values_for(keys)
+    t0 = time.time()
+    ref = po.RefTree(keys, vals)
+    build_s = time.time() - t0
+    m = min(1 << args.queries_log2, 1 << args.cpu_sample_log2)
+    q = dg.gen_point_queries(keys, 1 << args.queries_log2, args.hit, 2)[:m]
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        ref.search(q, threads)
+    times = []
+    for _ in range(args.steps):
+        a = time.perf_counter()
+        ref.search(q, threads)
+        times.append(time.perf_counter() - a)
+    sec = sum(times) / len(times)
+    v = m / sec / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded splitmix64 keys/queries)",
+        "config": {"workload": f"point search, 2^{args.keys_log2}-key tree, fanout {args.fanout} (reference "
+                               f"HB-style PPI tree, BPT_ORDER 64), 2^{args.queries_log2}-query batch, "
+                               f"{int(args.hit * 100)}% hits", "queries_per_step": m},
+        "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{m} of the batch's queries per step, OpenMP BPlusTree::search over "
+                                   f"{threads} threads; tree build {build_s:.0f} s excluded"},
+        "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_port(keys_sorted, vals_sorted, q, seconds: float = 10.0):
+    """The oracle's C restatement, single-threaded, on a bounded query sample."""
+    from oracle import pyoracle as po
+
+    t = po.PortTree(keys_sorted, vals_sorted)
+    m = 1 << 16
+    a = time.perf_counter()
+    done = 0
+    while done < len(q) and time.perf_counter() - a < seconds:
+        t.search(q[done:done + m])
+        done += m
+    sec = time.perf_counter() - a
+    return {"value": round(min(done, len(q)) / sec / 1e6, 3), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{min(done, len(q))} queries of the batch in {sec:.1f} s, scalar C restatement "
+                      f"(oracle/hm_oracle.c), 1 thread"}
+
+
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    from harmonia_b200 import BPlusTree, datagen as dg, launch_count
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+
+    n = 1 << args.keys_log2
+    m = 1 << args.queries_log2
+    keys = dg.gen_keys(n, 1)
+    vals = dg.values_for(keys)
+    q = dg.gen_point_queries(keys, m, args.hit, 2 + 1000 * rank)
+    d_keys = torch.from_numpy(keys).to(dev)
+    d_vals = torch.from_numpy(vals).to(dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tree = BPlusTree.bulk_load(d_keys, d_vals, fanout=args.fanout, leaf_cap=args.leaf_cap)
+    torch.cuda.synchronize()
+    bulk_ms = (time.perf_counter() - t0) * 1e3
+    del d_keys, d_vals
+    d_q = torch.from_numpy(q).to(dev)
+    d_out = torch.empty_like(d_q)
+    info = tree.info()
+
+    def timed(steps, fn):
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        ms = a.elapsed_time(b)
+        if ws > 1:
+            x = torch.tensor([ms], device=dev)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            ms = float(x.item())
+        return ms / steps
+
+    extras = {}
+    # plain single-batch launch: unsorted, default group width/depth, no tuning
+    if args.extras:
+        tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0)
+        for _ in range(args.warmup):
+            tree.search(d_q, d_out)
+        plain_ms = timed(args.steps, lambda: tree.search(d_q, d_out))
+        extras["plain"] = {"value": round(ws * m / plain_ms / 1e3, 1), "unit": UNIT, "ms_per_step": round(plain_ms, 4),
+                           "what": "one launch of the search kernel on the unsorted batch, group width 4, "
+                                   "2 queries per group, no pre-sort"}
+    tree.set_search_config(group_width=args.group_width, queries_per_group=args.qpg,
+                           sort_bits=args.sort_bits, cache_hints=args.hints)
+    tuned = tree.config()
+    if not args.no_tune:
+        tuned = tree.autotune(d_q)
+    for _ in range(args.warmup):
+        tree.search(d_q, d_out)
+    # spot check outside the timed region: a loaded key's value is
+    # splitmix64(key) >> 1 by construction of the workload, a miss is -1
+    sk = np.sort(keys)
+    qs = q[:4096]
+    pos = np.searchsorted(sk, qs).clip(max=n - 1)
+    exp = np.where(sk[pos] == qs, dg.values_for(qs), -1)
+    assert (d_out[:4096].cpu().numpy() == exp).all(), "search results are wrong"
+
+    # ---- headline timed region ----
+    tree.profile(True)
+    tree.profile_read()
+    l0 = launch_count()
+    with ClockSampler(local) as clk:
+        ms = timed(args.steps, lambda: tree.search(d_q, d_out))
+    launches = launch_count() - l0
+    stages = tree.profile_read()
+    tree.profile(False)
+    value = ws * m / ms / 1e3  # Mqueries/s (m queries per rank per step)
+
+    search_launches, search_total = stages.get("search", (0, 0.0))
+    search_ms = search_total / max(search_launches, 1)
+    peak, peak_kind = peaks()
+    bq = algorithmic_bytes_per_query(args.fanout)
+    achieved = bq * m / (search_ms * 1e-3) / 1e9 if search_ms > 0 else None
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(f"search_f{args.fanout}_lc{args.leaf_cap}_bits{tuned['sort_bits']}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": "search_kernel", "achieved": round(achieved, 1) if achieved else None,
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+                "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_query": bq, "queries_per_launch": m,
+                "kernel_ms": round(search_ms, 4)}
+
+    # pre-sorted input (the batch arrives partially sorted by its top 16 key bits)
+    if args.extras:
+        order = np.argsort(q >> np.int64(47), kind="stable")
+        d_qs = torch.from_numpy(q[order]).to(dev)
+        tree.set_search_config(sort_bits=0)
+        for _ in range(args.warmup):
+            tree.search(d_qs, d_out)
+        ps_ms = timed(args.steps, lambda: tree.search(d_qs, d_out))
+        extras["presorted_input"] = {"value": round(ws * m / ps_ms / 1e3, 1), "unit": UNIT,
+                                     "what": "batch pre-sorted by its top 16 key bits before the timed region"}
+        tree.set_search_config(**{k: tuned[k] for k in ("group_width", "queries_per_group", "sort_bits",
+                                                       "cache_hints")})
+        del d_qs
+
+    # ---- end to end through the public API with host (pinned) buffers ----
+    h_q = torch.from_numpy(q).pin_memory()
+    h_out = torch.empty_like(h_q).pin_memory()
+    for _ in range(args.warmup):
+        tree.search(h_q, h_out)
+    e2e_ms = timed(args.steps, lambda: tree.search(h_q, h_out))
+    assert (h_out[:4096].numpy() == exp).all()
+    e2e = {"value": round(ws * m / e2e_ms / 1e3, 1), "unit": UNIT, "h2d_bytes_per_step": m * 8,
+           "d2h_bytes_per_step": m * 8, "ms_per_step": round(e2e_ms, 3),
+           "what": "BPlusTree.search on pinned host buffers: chunked H2D, search, D2H through the C ABI"}
+
+    cpu = None
+    if rank == 0 and ws == 1:
+        cpu = cpu_baseline_port(sk, dg.values_for(sk), q, seconds=8.0)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded splitmix64 keys/queries)",
+            "config": {"workload": f"point search, 2^{args.keys_log2}-key tree, fanout {args.fanout}, "
+                                   f"leaf {args.leaf_cap}, one 2^{args.queries_log2}-query batch, "
+                                   f"{int(args.hit * 100)}% hits",
+                       "l2": "inputs larger than L2 (2^24 x 8 B queries + tree of "
+                             f"{info.device_bytes / 2**30:.2f} GiB), no flush",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                       "tuned": {k: tuned[k] for k in ("group_width", "queries_per_group", "sort_bits",
+                                                       "cache_hints")},
+                       "tree": {"height": info.height, "n_inner": info.n_inner, "n_leaf": info.n_leaf,
+                                "smem_levels": info.smem_levels},
+                       "bulk_load_ms": round(bulk_ms, 1)},
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+            "stages_ms_per_step": {k: round(v[1] / max(v[0], 1), 4) for k, v in stages.items()},
+            "roofline": roofline,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        line.update(extras)
+        if "plain" in extras:
+            line["vs_plain"] = round(value / extras["plain"]["value"], 3)
+        print(json.dumps(line), flush=True)
+    tree.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,808 @@
+// C-ABI entry points (include/harmonia.h) and the host-side orchestration:
+// argument checks, device/host pointer handling, the chunked copy pipeline
+// for host buffers, scratch management and error reporting.  The reference
+// drivers this replaces exit on any CUDA error
+// (CUDA_ERROR_HANDLER, open-harmonia/src/cuda_utils.h:3-12); every path here
+// returns an HM_E* code instead.
+#include "hm_internal.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace hm {
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
+int cuda_err(cudaError_t e) {
+  if (e == cudaSuccess) return HM_OK;
+  if (e == cudaErrorMemoryAllocation) return HM_ENOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return HM_ENODEVICE;
+  return HM_ECUDA;
+}
+
+int ensure_scratch(hm_tree *t, size_t bytes) {
+  if (bytes <= t->scratch_bytes) return HM_OK;
+  if (t->scratch) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_err(e);
+    cudaFree(t->scratch);
+    t->scratch = nullptr;
+    t->scratch_bytes = 0;
+  }
+  size_t want = (size_t)align_up((int64_t)bytes, 1 << 20);
+  cudaError_t e = cudaMalloc(&t->scratch, want);
+  if (e != cudaSuccess) {
+    t->scratch = nullptr;
+    return cuda_err(e);
+  }
+  t->scratch_bytes = want;
+  return HM_OK;
+}
+
+static const char *kStageNames[kStageCount] = {"partition", "search", "search_batches", "range",
+                                               "upsert"};
+
+static cudaEvent_t prof_event(hm_tree *t) {
+  if (!t->prof_pool.empty()) {
+    cudaEvent_t e = t->prof_pool.back();
+    t->prof_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+int prof_begin(hm_tree *t, cudaStream_t s) {
+  if (!t->prof) return -1;
+  hm_tree::ProfRec r{-1, prof_event(t), prof_event(t)};
+  cudaEventRecord(r.a, s);
+  t->prof_recs.push_back(r);
+  return (int)t->prof_recs.size() - 1;
+}
+
+void prof_end(hm_tree *t, int stage, int token, cudaStream_t s) {
+  if (token < 0 || token >= (int)t->prof_recs.size()) return;
+  t->prof_recs[token].stage = stage;
+  cudaEventRecord(t->prof_recs[token].b, s);
+}
+
+}  // namespace hm
+
+using namespace hm;
+
+namespace {
+
+constexpr int64_t kChunk = 1 << 22;  // queries per host-pipeline chunk
+
+bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+bool is_pinned_host(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+int check_config(const hm_config &c) {
+  if (c.fanout != 64 && c.fanout != 128) return HM_EINVAL;
+  if (c.leaf_cap != 16 && c.leaf_cap != 64) return HM_EINVAL;
+  if (c.inner_fill < 2 || c.inner_fill > c.fanout) return HM_EINVAL;
+  if (c.leaf_fill < 1 || c.leaf_fill > c.leaf_cap) return HM_EINVAL;
+  switch (c.group_width) {
+    case 1: case 2: case 4: case 8: case 16: case 32: break;
+    default: return HM_EINVAL;
+  }
+  if (c.queries_per_group != 1 && c.queries_per_group != 2 && c.queries_per_group != 4)
+    return HM_EINVAL;
+  if (c.sort_bits < -1 || c.sort_bits > 12) return HM_EINVAL;
+  if (c.smem_bytes < 0 || c.smem_bytes > 200 * 1024) return HM_EINVAL;
+  if (c.cache_hints != 1 && c.cache_hints != 2) return HM_EINVAL;
+  return HM_OK;
+}
+
+void fill_defaults(hm_config *c) {
+  if (c->fanout == 0) c->fanout = 64;
+  if (c->leaf_cap == 0) c->leaf_cap = 16;
+  if (c->inner_fill == 0) c->inner_fill = c->fanout;
+  if (c->leaf_fill == 0) c->leaf_fill = c->leaf_cap;
+  if (c->group_width == 0) c->group_width = 4;
+  if (c->queries_per_group == 0) c->queries_per_group = 2;
+  if (c->smem_bytes == 0) c->smem_bytes = 48 * 1024;
+  if (c->cache_hints == 0) c->cache_hints = 1;
+}
+
+void choose_smem_levels(hm_tree *t) {
+  t->smem_levels = 0;
+  t->smem_nodes = 0;
+  for (int l = 1; l <= t->height; l++) {
+    int64_t nodes = t->lvl_start[l];
+    int64_t bytes = nodes * t->inner_row * 8 + align_up(nodes * 4, 16) + 16;
+    if (bytes > t->cfg.smem_bytes) break;
+    t->smem_levels = l;
+    t->smem_nodes = (int)nodes;
+  }
+}
+
+// Effective pre-sort bits for a batch of n queries (0 = no pre-sort).
+int sort_bits_for(const hm_tree *t, int64_t n) {
+  if (n > INT32_MAX) return 0;  // positions are carried as int32
+  int b = t->cfg.sort_bits;
+  if (b >= 0) return b;
+  // auto: partition large batches only; 8 bits keeps >= 32 queries per
+  // bucket per partition CTA at the batch sizes where it pays.
+  return (n >= (1 << 21) && t->n_leaf >= (1 << 16)) ? 8 : 0;
+}
+
+cudaStream_t as_stream(hm_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int free_tree(hm_tree *t) {
+  if (!t) return HM_OK;
+  cudaDeviceSynchronize();
+  if (t->arena) cudaFree(t->arena);
+  if (t->scratch) cudaFree(t->scratch);
+  if (t->d_err) cudaFree(t->d_err);
+  if (t->pinned) cudaFreeHost(t->pinned);
+  for (auto &s : t->io_stream)
+    if (s) cudaStreamDestroy(s);
+  for (auto &e : t->io_event)
+    if (e) cudaEventDestroy(e);
+  for (auto &r : t->prof_recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto &e : t->prof_pool) cudaEventDestroy(e);
+  delete t;
+  return HM_OK;
+}
+
+int ensure_io(hm_tree *t) {
+  if (t->io_stream[0]) return HM_OK;
+  for (auto &s : t->io_stream) {
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_err(e);
+  }
+  for (auto &e : t->io_event) {
+    cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if (r != cudaSuccess) return cuda_err(r);
+  }
+  return HM_OK;
+}
+
+int ensure_pinned(hm_tree *t, size_t bytes) {
+  if (bytes <= t->pinned_bytes) return HM_OK;
+  if (t->pinned) cudaFreeHost(t->pinned);
+  t->pinned = nullptr;
+  t->pinned_bytes = 0;
+  cudaError_t e = cudaMallocHost(&t->pinned, bytes);
+  if (e != cudaSuccess) return cuda_err(e);
+  t->pinned_bytes = bytes;
+  return HM_OK;
+}
+
+// Search of device-resident queries on stream s, with the optional pre-sort.
+int search_device(hm_tree *t, const int64_t *d_q, int64_t n, int64_t *d_out, cudaStream_t s,
+                  void *scratch_base, size_t scratch_avail) {
+  int bits = sort_bits_for(t, n);
+  if (bits > 0) {
+    size_t need = (size_t)align_up(n * 8, 256) + (size_t)align_up(n * 4, 256) +
+                  partition_scratch_bytes(n, bits);
+    if (need <= scratch_avail) {
+      char *p = static_cast<char *>(scratch_base);
+      int64_t *qs = reinterpret_cast<int64_t *>(p);
+      int32_t *pos = reinterpret_cast<int32_t *>(p + align_up(n * 8, 256));
+      void *ps = p + align_up(n * 8, 256) + align_up(n * 4, 256);
+      int tok = prof_begin(t, s);
+      int rc = partition_queries(t, d_q, n, bits, qs, pos, ps, s);
+      prof_end(t, kStagePartition, tok, s);
+      if (rc) return rc;
+      SearchLaunch l{qs, d_out, pos, n};
+      tok = prof_begin(t, s);
+      rc = launch_search(t, l, t->cfg.group_width, t->cfg.queries_per_group, s);
+      prof_end(t, kStageSearch, tok, s);
+      return rc;
+    }
+  }
+  SearchLaunch l{d_q, d_out, nullptr, n};
+  int tok = prof_begin(t, s);
+  int rc = launch_search(t, l, t->cfg.group_width, t->cfg.queries_per_group, s);
+  prof_end(t, kStageSearch, tok, s);
+  return rc;
+}
+
+size_t search_scratch_need(const hm_tree *t, int64_t n) {
+  int bits = sort_bits_for(t, n);
+  if (bits <= 0) return 0;
+  return (size_t)align_up(n * 8, 256) + (size_t)align_up(n * 4, 256) +
+         partition_scratch_bytes(n, bits);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hm_config_default(hm_config *cfg) {
+  if (!cfg) return HM_EINVAL;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->sort_bits = -1;
+  fill_defaults(cfg);
+  return HM_OK;
+}
+
+const char *hm_strerror(int code) {
+  switch (code) {
+    case HM_OK: return "ok";
+    case HM_EINVAL: return "invalid argument or configuration";
+    case HM_ENOMEM: return "out of device or pinned host memory";
+    case HM_EDUPLICATE: return "bulk load: duplicate key";
+    case HM_EMAXKEY: return "key equals the sentinel INT64_MAX";
+    case HM_ECUDA: return "CUDA runtime error";
+    case HM_ECAPACITY: return "output capacity too small";
+    case HM_ETIMEOUT: return "a bounded device-side wait gave up";
+    case HM_ENODEVICE: return "no usable CUDA device";
+    case HM_EBUSY: return "busy: queue full or memory budget exhausted";
+    case HM_ECANCELLED: return "request cancelled or server stopped";
+    case HM_ETOOLARGE: return "size exceeds a documented maximum";
+    default: return "unknown error";
+  }
+}
+
+uint64_t hm_launch_count(void) { return g_launches.load(); }
+
+int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_config *cfg_in,
+                 hm_tree **out) {
+  if (!out || (n_ > 0 && (!keys || !vals))) return HM_EINVAL;
+  *out = nullptr;
+  hm_config cfg;
+  if (cfg_in) {
+    cfg = *cfg_in;
+    fill_defaults(&cfg);
+  } else {
+    hm_config_default(&cfg);
+  }
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  const int64_t n = (int64_t)n_;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_err(e);
+
+  hm_tree *t = new (std::nothrow) hm_tree();
+  if (!t) return HM_ENOMEM;
+  t->device = dev;
+  t->cfg = cfg;
+  cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  rc = shape(n, cfg, &t->height, t->lvl_start, &t->n_inner, &t->n_leaf);
+  if (rc) {
+    delete t;
+    return rc;
+  }
+  t->n_keys = n;
+  t->inner_row = cfg.fanout / 8 + cfg.fanout;
+  t->leaf_index = cfg.leaf_cap >= 32 ? cfg.leaf_cap / 8 : 0;
+  t->leaf_row = t->leaf_index + cfg.leaf_cap;
+
+  // Arena: every array 256-B aligned; prefix padded to a multiple of 4.
+  size_t off_inner = 0;
+  size_t off_prefix = off_inner + align_up(t->n_inner * t->inner_row * 8, 256);
+  size_t off_lkeys = off_prefix + align_up(align_up(t->n_inner, 4) * 4, 256);
+  size_t off_lvals = off_lkeys + align_up(t->n_leaf * t->leaf_row * 8, 256);
+  size_t off_lcnt = off_lvals + align_up(t->n_leaf * cfg.leaf_cap * 8, 256);
+  size_t off_lbase = off_lcnt + align_up(t->n_leaf * 4, 256);
+  size_t total = off_lbase + align_up(t->n_leaf * 8, 256);
+
+  // Temporaries: two key and two value buffers for the sort, sort scratch, flags.
+  int64_t tn = std::max<int64_t>(std::max<int64_t>(n, t->n_leaf), 1);
+  size_t tb = align_up(tn * 8, 256);
+  size_t temp_bytes = 4 * tb + align_up((int64_t)radix_scratch_bytes(n), 256) + 256;
+  char *temp = nullptr;
+  e = cudaMalloc(&t->arena, total);
+  if (e == cudaSuccess) e = cudaMalloc(&temp, temp_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&t->d_err, 256);
+  if (e != cudaSuccess) {
+    if (temp) cudaFree(temp);
+    free_tree(t);
+    return cuda_err(e);
+  }
+  t->arena_bytes = total;
+  char *base = static_cast<char *>(t->arena);
+  t->inner = reinterpret_cast<int64_t *>(base + off_inner);
+  t->prefix = reinterpret_cast<int32_t *>(base + off_prefix);
+  t->leaf_keys = reinterpret_cast<int64_t *>(base + off_lkeys);
+  t->leaf_vals = reinterpret_cast<int64_t *>(base + off_lvals);
+  t->leaf_cnt = reinterpret_cast<int32_t *>(base + off_lcnt);
+  t->leaf_base = reinterpret_cast<int64_t *>(base + off_lbase);
+
+  uint64_t *uk = reinterpret_cast<uint64_t *>(temp);
+  uint64_t *uk_alt = reinterpret_cast<uint64_t *>(temp + tb);
+  int64_t *vv = reinterpret_cast<int64_t *>(temp + 2 * tb);
+  int64_t *vv_alt = reinterpret_cast<int64_t *>(temp + 3 * tb);
+  void *sort_scratch = temp + 4 * tb;
+  unsigned *flags = reinterpret_cast<unsigned *>(temp + temp_bytes - 256);
+  cudaStream_t s = 0;
+  cudaMemsetAsync(t->arena, 0, total, s);
+  cudaMemsetAsync(t->d_err, 0, 256, s);
+  cudaMemsetAsync(flags, 0, 4, s);
+  if (n > 0) {
+    // keys land in uk_alt as int64, are sign-flipped into uk, values go to vv
+    e = cudaMemcpyAsync(uk_alt, keys, n * 8, cudaMemcpyDefault, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vv, vals, n * 8, cudaMemcpyDefault, s);
+    if (e != cudaSuccess) {
+      cudaFree(temp);
+      free_tree(t);
+      return cuda_err(e);
+    }
+    transform_keys_in(reinterpret_cast<int64_t *>(uk_alt), uk, n, s);
+    bool alt = radix_sort_pairs<int64_t>(uk, vv, uk_alt, vv_alt, n, 0, 64, sort_scratch, s);
+    if (alt) {
+      std::swap(uk, uk_alt);
+      std::swap(vv, vv_alt);
+    }
+    check_sorted_keys(uk, n, flags, s);
+  }
+  unsigned hflags = 0;
+  e = cudaMemcpyAsync(&hflags, flags, 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess || hflags) {
+    cudaFree(temp);
+    free_tree(t);
+    if (e != cudaSuccess) return cuda_err(e);
+    return (hflags & 2u) ? HM_EMAXKEY : HM_EDUPLICATE;
+  }
+  rc = build_from_sorted(t, uk, vv, n, reinterpret_cast<int64_t *>(uk_alt), vv_alt, s);
+  if (rc == HM_OK && n > 0) {
+    uint64_t ends[2] = {0, 0};
+    cudaMemcpyAsync(&ends[0], uk, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&ends[1], uk + n - 1, 8, cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    t->key_min = (int64_t)(ends[0] ^ kSign);
+    t->key_max = (int64_t)(ends[1] ^ kSign);
+    if (e != cudaSuccess) rc = cuda_err(e);
+  } else if (rc == HM_OK) {
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = cuda_err(e);
+  }
+  cudaFree(temp);
+  if (rc) {
+    free_tree(t);
+    return rc;
+  }
+  choose_smem_levels(t);
+  *out = t;
+  return HM_OK;
+}
+
+int hm_free(hm_tree *t) { return free_tree(t); }
+
+int hm_tree_get_info(const hm_tree *t, hm_tree_info *info) {
+  if (!t || !info) return HM_EINVAL;
+  std::memset(info, 0, sizeof(*info));
+  info->fanout = t->cfg.fanout;
+  info->leaf_cap = t->cfg.leaf_cap;
+  info->height = t->height;
+  info->inner_row_words = t->inner_row;
+  info->leaf_row_words = t->leaf_row;
+  info->leaf_index_words = t->leaf_index;
+  info->smem_levels = t->smem_levels;
+  info->n_keys = t->n_keys;
+  info->n_inner = t->n_inner;
+  info->n_leaf = t->n_leaf;
+  for (int i = 0; i <= t->height && i <= kMaxLevels; i++) info->lvl_start[i] = t->lvl_start[i];
+  info->inner = t->inner;
+  info->prefix = t->prefix;
+  info->leaf_keys = t->leaf_keys;
+  info->leaf_vals = t->leaf_vals;
+  info->leaf_cnt = t->leaf_cnt;
+  info->leaf_base = t->leaf_base;
+  info->device_bytes = t->arena_bytes;
+  return HM_OK;
+}
+
+int hm_get_config(const hm_tree *t, hm_config *cfg) {
+  if (!t || !cfg) return HM_EINVAL;
+  *cfg = t->cfg;
+  return HM_OK;
+}
+
+int hm_set_search_config(hm_tree *t, const hm_config *cfg) {
+  if (!t || !cfg) return HM_EINVAL;
+  hm_config c = t->cfg;
+  if (cfg->group_width) c.group_width = cfg->group_width;
+  if (cfg->queries_per_group) c.queries_per_group = cfg->queries_per_group;
+  c.sort_bits = cfg->sort_bits;
+  if (cfg->smem_bytes) c.smem_bytes = cfg->smem_bytes;
+  if (cfg->cache_hints) c.cache_hints = cfg->cache_hints;
+  int rc = check_config(c);
+  if (rc) return rc;
+  t->cfg = c;
+  choose_smem_levels(t);
+  return HM_OK;
+}
+
+int hm_search(hm_tree *t, const int64_t *q, size_t n_, int64_t *out, hm_stream hs) {
+  if (!t || (n_ > 0 && (!q || !out))) return HM_EINVAL;
+  const int64_t n = (int64_t)n_;
+  if (n == 0) return HM_OK;
+  cudaStream_t s = as_stream(hs);
+  bool dq = is_device_ptr(q), dout = is_device_ptr(out);
+  if (dq && dout) {
+    int rc = ensure_scratch(t, search_scratch_need(t, n));
+    if (rc) return rc;
+    return search_device(t, q, n, out, s, t->scratch, t->scratch_bytes);
+  }
+  if (dq != dout) return HM_EINVAL;  // mixed host/device buffers are not supported
+  // Host buffers: chunked pipeline, copies on two streams overlapping the search.
+  int rc = ensure_io(t);
+  if (rc) return rc;
+  const int64_t chunk = std::min<int64_t>(kChunk, n);
+  const size_t cbytes = (size_t)align_up(chunk * 8, 256);
+  const size_t sneed = search_scratch_need(t, chunk);
+  rc = ensure_scratch(t, 4 * cbytes + sneed);
+  if (rc) return rc;
+  char *sb = static_cast<char *>(t->scratch);
+  int64_t *dqb[2] = {reinterpret_cast<int64_t *>(sb), reinterpret_cast<int64_t *>(sb + cbytes)};
+  int64_t *dob[2] = {reinterpret_cast<int64_t *>(sb + 2 * cbytes),
+                     reinterpret_cast<int64_t *>(sb + 3 * cbytes)};
+  void *search_scratch = sb + 4 * cbytes;
+  const bool pinned = is_pinned_host(q) && is_pinned_host(out);
+  int64_t *hq[2] = {nullptr, nullptr}, *ho[2] = {nullptr, nullptr};
+  if (!pinned) {
+    rc = ensure_pinned(t, 4 * cbytes);
+    if (rc) return rc;
+    char *pb = static_cast<char *>(t->pinned);
+    hq[0] = reinterpret_cast<int64_t *>(pb);
+    hq[1] = reinterpret_cast<int64_t *>(pb + cbytes);
+    ho[0] = reinterpret_cast<int64_t *>(pb + 2 * cbytes);
+    ho[1] = reinterpret_cast<int64_t *>(pb + 3 * cbytes);
+  }
+  cudaStream_t sin = t->io_stream[0], scomp = t->io_stream[1], sout = t->io_stream[2];
+  cudaEvent_t *ev_in = t->io_event, *ev_comp = t->io_event + 2, *ev_out = t->io_event + 4;
+  // Order the pipeline after prior work on the caller's stream.
+  cudaEventRecord(t->io_event[6], s);
+  cudaStreamWaitEvent(sin, t->io_event[6], 0);
+  cudaStreamWaitEvent(scomp, t->io_event[6], 0);
+  const int64_t nchunks = (n + chunk - 1) / chunk;
+  cudaError_t e = cudaSuccess;
+  for (int64_t c = 0; c < nchunks && e == cudaSuccess; c++) {
+    const int b = (int)(c & 1);
+    const int64_t o = c * chunk, m = std::min(chunk, n - o);
+    if (c >= 2) cudaStreamWaitEvent(sin, ev_comp[b], 0);  // dqb[b] no longer read
+    if (pinned) {
+      e = cudaMemcpyAsync(dqb[b], q + o, m * 8, cudaMemcpyHostToDevice, sin);
+    } else {
+      if (c >= 2) cudaEventSynchronize(ev_in[b]);  // staging hq[b] consumed
+      std::memcpy(hq[b], q + o, m * 8);
+      e = cudaMemcpyAsync(dqb[b], hq[b], m * 8, cudaMemcpyHostToDevice, sin);
+    }
+    cudaEventRecord(ev_in[b], sin);
+    cudaStreamWaitEvent(scomp, ev_in[b], 0);
+    if (c >= 2) cudaStreamWaitEvent(scomp, ev_out[b], 0);  // dob[b] drained
+    rc = search_device(t, dqb[b], m, dob[b], scomp, search_scratch, sneed);
+    if (rc) break;
+    cudaEventRecord(ev_comp[b], scomp);
+    cudaStreamWaitEvent(sout, ev_comp[b], 0);
+    if (pinned) {
+      e = cudaMemcpyAsync(out + o, dob[b], m * 8, cudaMemcpyDeviceToHost, sout);
+      cudaEventRecord(ev_out[b], sout);
+    } else {
+      if (c >= 2) {
+        // drain chunk c-2 from staging before reusing ho[b]
+        cudaEventSynchronize(ev_out[b]);
+        const int64_t po = (c - 2) * chunk, pm = std::min(chunk, n - po);
+        std::memcpy(out + po, ho[b], pm * 8);
+      }
+      e = cudaMemcpyAsync(ho[b], dob[b], m * 8, cudaMemcpyDeviceToHost, sout);
+      cudaEventRecord(ev_out[b], sout);
+    }
+  }
+  if (rc == HM_OK && e == cudaSuccess) e = cudaStreamSynchronize(sout);
+  if (rc == HM_OK && e == cudaSuccess && !pinned) {
+    for (int64_t c = std::max<int64_t>(0, nchunks - 2); c < nchunks; c++) {
+      const int b = (int)(c & 1);
+      const int64_t po = c * chunk, pm = std::min(chunk, n - po);
+      std::memcpy(out + po, ho[b], pm * 8);
+    }
+  }
+  cudaStreamSynchronize(scomp);
+  cudaStreamSynchronize(sin);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_err(e);
+  return hm_sync(t, hs);
+}
+
+int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream hs) {
+  if (!t || nb < 0 || (nb > 0 && !batches)) return HM_EINVAL;
+  if (nb == 0) return HM_OK;
+  cudaStream_t s = as_stream(hs);
+  const int tileq = search_tile_queries(t->cfg.group_width, t->cfg.queries_per_group);
+  std::vector<int64_t> ts((size_t)nb + 2);
+  ts[0] = 0;
+  for (int i = 0; i < nb; i++) {
+    if (batches[i].n < 0 || (batches[i].n > 0 && (!batches[i].q || !batches[i].out)))
+      return HM_EINVAL;
+    ts[i + 1] = ts[i] + (batches[i].n + tileq - 1) / tileq;
+  }
+  ts[nb + 1] = 0;  // tile counter
+  size_t bbytes = align_up((int64_t)sizeof(hm_batch) * nb, 256);
+  size_t tbytes = align_up((int64_t)sizeof(int64_t) * (nb + 2), 256);
+  int rc = ensure_scratch(t, bbytes + tbytes);
+  if (rc) return rc;
+  char *sb = static_cast<char *>(t->scratch);
+  hm_batch *d_b = reinterpret_cast<hm_batch *>(sb);
+  int64_t *d_ts = reinterpret_cast<int64_t *>(sb + bbytes);
+  cudaError_t e = cudaMemcpyAsync(d_b, batches, sizeof(hm_batch) * nb, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_ts, ts.data(), sizeof(int64_t) * (nb + 2), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return cuda_err(e);
+  // The host arrays must stay valid until the copies finish.
+  int tok = prof_begin(t, s);
+  rc = launch_search_batches(t, d_b, d_ts, nb, ts[nb], t->cfg.group_width,
+                             t->cfg.queries_per_group, s);
+  prof_end(t, kStageBatches, tok, s);
+  e = cudaStreamSynchronize(s);
+  if (rc) return rc;
+  return cuda_err(e);
+}
+
+int hm_sync(hm_tree *t, hm_stream hs) {
+  if (!t) return HM_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(as_stream(hs));
+  if (e != cudaSuccess) return cuda_err(e);
+  unsigned err = 0;
+  e = cudaMemcpy(&err, t->d_err, 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_err(e);
+  if (err) {
+    cudaMemset(t->d_err, 0, 4);
+    return (err & kErrTimeout) ? HM_ETIMEOUT : HM_ECUDA;
+  }
+  return HM_OK;
+}
+
+int hm_export(hm_tree *t, int64_t *keys, int64_t *vals, size_t cap, size_t *n) {
+  if (!t) return HM_EINVAL;
+  if (n) *n = (size_t)t->n_keys;
+  if ((size_t)t->n_keys > cap) return HM_ECAPACITY;
+  if (t->n_keys == 0) return HM_OK;
+  if (!keys || !vals) return HM_EINVAL;
+  cudaStream_t s = 0;
+  bool dk = is_device_ptr(keys), dv = is_device_ptr(vals);
+  if (dk && dv) {
+    export_contents(t, keys, vals, s);
+    return cuda_err(cudaStreamSynchronize(s));
+  }
+  const size_t b = (size_t)align_up(t->n_keys * 8, 256);
+  int rc = ensure_scratch(t, 2 * b);
+  if (rc) return rc;
+  int64_t *ek = static_cast<int64_t *>(t->scratch);
+  int64_t *ev = reinterpret_cast<int64_t *>(static_cast<char *>(t->scratch) + b);
+  export_contents(t, ek, ev, s);
+  cudaError_t e = cudaMemcpyAsync(keys, ek, t->n_keys * 8, cudaMemcpyDefault, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vals, ev, t->n_keys * 8, cudaMemcpyDefault, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return cuda_err(e);
+}
+
+int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n_, int64_t *offsets,
+             int64_t *okeys, int64_t *ovals, size_t cap, size_t *total, hm_stream hs) {
+  if (!t || (n_ > 0 && (!start || !len)) || !offsets) return HM_EINVAL;
+  const int64_t n = (int64_t)n_;
+  cudaStream_t s = as_stream(hs);
+  if (total) *total = 0;
+  const bool dev_in = n == 0 || (is_device_ptr(start) && is_device_ptr(len));
+  const bool dev_out = is_device_ptr(offsets);
+  const size_t b8 = (size_t)align_up((n + 1) * 8, 256), b4 = (size_t)align_up(n * 4 + 4, 256);
+  size_t need = 2 * b4 + b8 + (size_t)align_up((int64_t)scan_scratch_bytes(n + 1), 256);
+  if (!dev_in) need += b8 + b4;
+  if (!dev_out) need += b8;
+  int rc = ensure_scratch(t, need);
+  if (rc) return rc;
+  char *p = static_cast<char *>(t->scratch);
+  int32_t *fl = reinterpret_cast<int32_t *>(p);
+  p += b4;
+  int32_t *fs = reinterpret_cast<int32_t *>(p);
+  p += b4;
+  int64_t *cnt = reinterpret_cast<int64_t *>(p);
+  p += b8;
+  void *scan_scratch = p;
+  p += align_up((int64_t)scan_scratch_bytes(n + 1), 256);
+  const int64_t *d_start = start;
+  const int32_t *d_len = len;
+  cudaError_t e = cudaSuccess;
+  if (!dev_in) {
+    int64_t *ds = reinterpret_cast<int64_t *>(p);
+    p += b8;
+    int32_t *dl = reinterpret_cast<int32_t *>(p);
+    p += b4;
+    e = cudaMemcpyAsync(ds, start, n * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dl, len, n * 4, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_err(e);
+    d_start = ds;
+    d_len = dl;
+  }
+  int64_t *d_off = dev_out ? offsets : reinterpret_cast<int64_t *>(p);
+  const int tok = prof_begin(t, s);
+  if (n > 0) {
+    rc = range_locate(t, d_start, d_len, n, fl, fs, cnt, s);
+    if (rc) return rc;
+  }
+  exclusive_scan_i64(cnt, d_off, n, scan_scratch, s);
+  int64_t tot = 0;
+  e = cudaMemcpyAsync(&tot, d_off + n, 8, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_err(e);
+  if (total) *total = (size_t)tot;
+  if (!dev_out) {
+    e = cudaMemcpy(offsets, d_off, (n + 1) * 8, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_err(e);
+  }
+  if ((size_t)tot > cap) return HM_ECAPACITY;
+  if (tot == 0) return HM_OK;
+  if (!okeys || !ovals) return HM_EINVAL;
+  const bool dev_rec = is_device_ptr(okeys) && is_device_ptr(ovals);
+  if (dev_rec) {
+    rc = range_copy_out(t, fl, fs, d_off, n, okeys, ovals, s);
+    prof_end(t, kStageRange, tok, s);
+    if (rc) return rc;
+    return hm_sync(t, hs);
+  }
+  int64_t *tk = nullptr;
+  e = cudaMalloc(&tk, 2 * (size_t)align_up(tot * 8, 256));
+  if (e != cudaSuccess) return cuda_err(e);
+  int64_t *tv = reinterpret_cast<int64_t *>(reinterpret_cast<char *>(tk) + align_up(tot * 8, 256));
+  rc = range_copy_out(t, fl, fs, d_off, n, tk, tv, s);
+  prof_end(t, kStageRange, tok, s);
+  if (rc == HM_OK) {
+    e = cudaMemcpyAsync(okeys, tk, tot * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ovals, tv, tot * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    rc = cuda_err(e);
+  }
+  cudaFree(tk);
+  return rc ? rc : hm_sync(t, hs);
+}
+
+int hm_upsert_batch(hm_tree *t, const int64_t *keys, const int64_t *vals, size_t n_, int flags,
+                    hm_stream hs) {
+  if (!t || (n_ > 0 && (!keys || !vals))) return HM_EINVAL;
+  if (flags != HM_UPSERT_SUPPLIED && flags != HM_UPSERT_REF_KEY_MINUS_1) return HM_EINVAL;
+  const int64_t n = (int64_t)n_;
+  if (n == 0) return HM_OK;
+  cudaStream_t s = as_stream(hs);
+  const int64_t *dk = keys, *dv = vals;
+  int64_t *tmp = nullptr;
+  if (!(is_device_ptr(keys) && is_device_ptr(vals))) {
+    cudaError_t e = cudaMalloc(&tmp, 2 * (size_t)align_up(n * 8, 256));
+    if (e != cudaSuccess) return cuda_err(e);
+    int64_t *tv = reinterpret_cast<int64_t *>(reinterpret_cast<char *>(tmp) + align_up(n * 8, 256));
+    e = cudaMemcpyAsync(tmp, keys, n * 8, cudaMemcpyDefault, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tv, vals, n * 8, cudaMemcpyDefault, s);
+    if (e != cudaSuccess) {
+      cudaFree(tmp);
+      return cuda_err(e);
+    }
+    dk = tmp;
+    dv = tv;
+  }
+  int tok = prof_begin(t, s);
+  int rc = upsert_epoch(t, dk, dv, n, flags, s);
+  prof_end(t, kStageUpsert, tok, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (tmp) cudaFree(tmp);
+  if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
+  choose_smem_levels(t);
+  return rc ? rc : hm_sync(t, hs);
+}
+
+int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n_, hm_config *best) {
+  if (!t || (n_ > 0 && !sample_q)) return HM_EINVAL;
+  const int64_t n = (int64_t)n_;
+  if (n == 0 || !is_device_ptr(sample_q)) return HM_EINVAL;
+  int64_t *d_out = nullptr;
+  cudaError_t e = cudaMalloc(&d_out, n * 8);
+  if (e != cudaSuccess) return cuda_err(e);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const hm_config orig = t->cfg;
+  hm_config best_cfg = orig;
+  float best_ms = 1e30f;
+  const int widths[] = {2, 4, 8, 16, 32};
+  const int qpgs[] = {1, 2, 4};
+  const int bits_list[] = {0, 6, 8, 10};
+  const int hints_list[] = {1, 2};
+  int rc = HM_OK;
+  for (int w : widths)
+    for (int q : qpgs)
+      for (int bits : bits_list)
+        for (int hints : hints_list) {
+        hm_config c = orig;
+        c.group_width = w;
+        c.queries_per_group = q;
+        c.sort_bits = bits;
+        c.cache_hints = hints;
+        t->cfg = c;
+        choose_smem_levels(t);
+        rc = ensure_scratch(t, search_scratch_need(t, n));
+        if (rc) break;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3 && rc == HM_OK; rep++) {
+          cudaEventRecord(a, 0);
+          rc = search_device(t, sample_q, n, d_out, 0, t->scratch, t->scratch_bytes);
+          cudaEventRecord(b, 0);
+          cudaEventSynchronize(b);
+          float x = 0;
+          cudaEventElapsedTime(&x, a, b);
+          if (rep > 0 && x < ms) ms = x;
+        }
+        if (rc) break;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_cfg = c;
+        }
+      }
+  t->cfg = rc ? orig : best_cfg;
+  choose_smem_levels(t);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(d_out);
+  if (best) *best = t->cfg;
+  return rc ? rc : hm_sync(t, 0);
+}
+
+int hm_profile(hm_tree *t, int enable) {
+  if (!t) return HM_EINVAL;
+  t->prof = enable != 0;
+  return HM_OK;
+}
+
+int hm_profile_read(hm_tree *t, hm_stage_time *out, int cap, int *n) {
+  if (!t || (cap > 0 && !out)) return HM_EINVAL;
+  double ms[kStageCount] = {};
+  uint64_t cnt[kStageCount] = {};
+  int rc = HM_OK;
+  for (auto &r : t->prof_recs) {
+    if (r.stage >= 0) {
+      cudaError_t e = cudaEventSynchronize(r.b);
+      float x = 0;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&x, r.a, r.b);
+      if (e != cudaSuccess) rc = cuda_err(e);
+      ms[r.stage] += x;
+      cnt[r.stage]++;
+    }
+    t->prof_pool.push_back(r.a);
+    t->prof_pool.push_back(r.b);
+  }
+  t->prof_recs.clear();
+  int k = 0;
+  for (int i = 0; i < kStageCount; i++) {
+    if (!cnt[i]) continue;
+    if (k < cap) {
+      std::memset(&out[k], 0, sizeof(out[k]));
+      std::strncpy(out[k].name, kStageNames[i], sizeof(out[k].name) - 1);
+      out[k].launches = cnt[i];
+      out[k].total_ms = ms[i];
+    }
+    k++;
+  }
+  if (n) *n = k;
+  return rc;
+}
+
+}  // extern "C"

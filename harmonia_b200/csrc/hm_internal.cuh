@@ -1,0 +1,195 @@
+// Internal definitions shared by the harmonia-b200 CUDA sources.
+//
+// Device layout of a tree (all in one HBM arena, every array 256-B aligned):
+//   inner     n_inner rows of (F/8 + F) int64: an index of every 8th key
+//             (index[j] = key[8(j+1)], Max_Key past the end) followed by F
+//             key slots, <= F-1 separators, Max_Key in unused slots.  Rows are
+//             numbered breadth-first, the root is row 0.  This is the
+//             reference's Inner_node key part (inner_index + inner_key,
+//             open-harmonia/src/bpt.h:76-80) in the CFB's BFS order
+//             (open-harmonia/regular_bpt/traversal.cpp:36-78).
+//   prefix    n_inner int32 (padded to a multiple of 4): id of the node's first
+//             child; children are contiguous, so child c of node i is
+//             prefix[i] + c.  Children of the last inner level are numbered
+//             from n_inner, leaf j = id - n_inner (CFB prefix[] and
+//             idx - internal_node_num, open-harmonia/regular_bpt/cfb.cpp:21-32).
+//   leaf_keys n_leaf rows of (LI + LC) int64, LI = LC/8 index words when
+//             LC >= 32 (else 0), then LC key slots.
+//   leaf_vals n_leaf * LC int64, -1 in unused slots.
+//   leaf_cnt  n_leaf int32 keys per leaf; leaf_base n_leaf int64 exclusive scan.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/harmonia.h"
+
+namespace hm {
+
+constexpr int64_t kMaxKey = INT64_MAX;
+constexpr uint64_t kSign = 0x8000000000000000ull;
+constexpr int kMaxLevels = 32;
+
+// Error word bits a kernel may set (read back by hm_sync).
+enum : unsigned {
+  kErrTimeout = 1u,   // a bounded mbarrier wait gave up
+  kErrBadNode = 2u,   // a node id fell outside the tree (corrupt layout)
+};
+
+struct DevTree {
+  const int64_t *inner;
+  const int32_t *prefix;
+  const int64_t *leaf_keys;
+  const int64_t *leaf_vals;
+  const int32_t *leaf_cnt;
+  const int64_t *leaf_base;
+  int64_t n_keys;
+  int32_t n_inner;
+  int32_t n_leaf;
+  int32_t height;      // inner levels
+  int32_t smem_nodes;  // top nodes staged in shared memory (a BFS prefix)
+  int32_t smem_levels;
+  int32_t cache_hints; // 1: L2 evict_last for inner rows, evict_first for leaves
+};
+
+__host__ __device__ inline int64_t part_start(int64_t j, int64_t total, int64_t parts) {
+  int64_t q = total / parts, r = total % parts;
+  return j * q + (j < r ? j : r);
+}
+
+inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+// Counts kernel launches issued by this library (hm_launch_count).
+void note_launch(int n = 1);
+
+}  // namespace hm
+
+struct hm_tree {
+  int device = 0;
+  hm_config cfg{};
+  int height = 0;
+  int inner_row = 0, leaf_row = 0, leaf_index = 0;
+  int64_t n_keys = 0, n_inner = 0, n_leaf = 0;
+  int64_t lvl_start[hm::kMaxLevels + 1] = {};
+  int smem_levels = 0;
+  int smem_nodes = 0;
+  int num_sms = 148;
+  int64_t key_min = 0, key_max = 0;  // for the pre-sort digit
+  // arena
+  void *arena = nullptr;
+  size_t arena_bytes = 0;
+  int64_t *inner = nullptr;
+  int32_t *prefix = nullptr;
+  int64_t *leaf_keys = nullptr;
+  int64_t *leaf_vals = nullptr;
+  int32_t *leaf_cnt = nullptr;
+  int64_t *leaf_base = nullptr;
+  // per-tree scratch (grown on demand), error word, pinned staging
+  void *scratch = nullptr;
+  size_t scratch_bytes = 0;
+  unsigned *d_err = nullptr;
+  void *pinned = nullptr;
+  size_t pinned_bytes = 0;
+  cudaStream_t io_stream[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t io_event[8] = {};
+  // stage timing (hm_profile): event pairs recorded around each stage
+  struct ProfRec {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  bool prof = false;
+  std::vector<ProfRec> prof_recs;
+  std::vector<cudaEvent_t> prof_pool;
+
+  hm::DevTree view() const {
+    hm::DevTree d;
+    d.inner = inner;
+    d.prefix = prefix;
+    d.leaf_keys = leaf_keys;
+    d.leaf_vals = leaf_vals;
+    d.leaf_cnt = leaf_cnt;
+    d.leaf_base = leaf_base;
+    d.n_keys = n_keys;
+    d.n_inner = (int32_t)n_inner;
+    d.n_leaf = (int32_t)n_leaf;
+    d.height = height;
+    d.smem_nodes = smem_nodes;
+    d.smem_levels = smem_levels;
+    d.cache_hints = cfg.cache_hints;
+    return d;
+  }
+};
+
+namespace hm {
+
+// ---- radix sort (sort.cu) ----
+// Stable LSD sort of (ukeys, vals) by bits [begin_bit, end_bit) of the
+// unsigned key.  Buffers ping-pong; returns true if the result ends in the
+// *_alt buffers.  Scratch needs radix_scratch_bytes(n).
+size_t radix_scratch_bytes(int64_t n);
+template <typename V>
+bool radix_sort_pairs(uint64_t *ukeys, V *vals, uint64_t *ukeys_alt, V *vals_alt,
+                      int64_t n, int begin_bit, int end_bit, void *scratch,
+                      cudaStream_t s);
+
+// ---- bulk build (build.cu) ----
+int shape(int64_t n, const hm_config &c, int *height, int64_t *lvl_start,
+          int64_t *n_inner, int64_t *n_leaf);
+// Builds the tree arrays of t (already sized and allocated) from sorted
+// unsigned-transformed keys; writes flags (bit0 dup, bit1 maxkey) to d_flags.
+int build_from_sorted(hm_tree *t, const uint64_t *ukeys, const int64_t *vals,
+                      int64_t n, int64_t *tmp_a, int64_t *tmp_b, cudaStream_t s);
+void check_sorted_keys(const uint64_t *ukeys, int64_t n, unsigned *d_flags, cudaStream_t s);
+void transform_keys_in(const int64_t *keys, uint64_t *ukeys, int64_t n, cudaStream_t s);
+void transform_keys_out(const uint64_t *ukeys, int64_t *keys, int64_t n, cudaStream_t s);
+
+// ---- search (search.cu) ----
+struct SearchLaunch {
+  const int64_t *q;
+  int64_t *out;
+  const int32_t *pos;  // optional: out[pos[i]] = result of q[i]
+  int64_t n;
+};
+int launch_search(const hm_tree *t, const SearchLaunch &l, int group_width, int qpg,
+                  cudaStream_t s);
+int launch_search_batches(const hm_tree *t, const hm_batch *d_batches, const int64_t *d_tile_start,
+                          int nb, int64_t total_tiles, int group_width, int qpg,
+                          cudaStream_t s);
+int search_tile_queries(int group_width, int qpg);  // queries per CTA tile
+size_t search_smem_bytes(const hm_tree *t);
+
+// ---- query pre-sort (partition.cu) ----
+size_t partition_scratch_bytes(int64_t n, int bits);
+int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits,
+                      int64_t *q_out, int32_t *pos_out, void *scratch, cudaStream_t s);
+
+// ---- scan, export, range (misc.cu) ----
+void scan_counts(int64_t *counts, int64_t m, cudaStream_t s);  // one-CTA in-place exclusive scan
+size_t scan_scratch_bytes(int64_t n);
+void exclusive_scan_i64(const int64_t *in, int64_t *out, int64_t n, void *scratch,
+                        cudaStream_t s);  // out has n+1 entries
+void exclusive_scan_i32(const int32_t *in, int64_t *out, int64_t n, void *scratch, cudaStream_t s);
+void export_contents(const hm_tree *t, int64_t *d_keys, int64_t *d_vals, cudaStream_t s);
+size_t range_scratch_bytes(int64_t n);
+int range_locate(const hm_tree *t, const int64_t *start, const int32_t *len, int64_t n,
+                 int32_t *first_leaf, int32_t *first_slot, int64_t *count, cudaStream_t s);
+int range_copy_out(const hm_tree *t, const int32_t *first_leaf, const int32_t *first_slot,
+                   const int64_t *offsets, int64_t n, int64_t *okeys, int64_t *ovals, cudaStream_t s);
+
+// ---- upsert (upsert.cu) ----
+int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64_t n,
+                 int flags, cudaStream_t s);
+
+// ---- stage timing ----
+enum Stage { kStagePartition = 0, kStageSearch, kStageBatches, kStageRange, kStageUpsert, kStageCount };
+// Records the start event of a stage on stream s (no-op unless profiling).
+int prof_begin(hm_tree *t, cudaStream_t s);
+void prof_end(hm_tree *t, int stage, int token, cudaStream_t s);
+
+// ---- misc ----
+int ensure_scratch(hm_tree *t, size_t bytes);
+int cuda_err(cudaError_t e);
+
+}  // namespace hm

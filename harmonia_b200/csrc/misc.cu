@@ -1,0 +1,237 @@
+// Device-wide exclusive scan, export of the tree contents, and the range scan
+// with prefix-sum output compaction.
+//
+// Range reference: range_prefix_sort_1thread_search_1_thread_scan_kernel
+// (open-harmonia/src/range.cu:101-227) descends with the start key and copies
+// up to Range_Size = 8 records into fixed per-query slots (no compaction),
+// with the end key forced to Max_Key (open-harmonia/src/range.cu:349-355).
+// Here a query asks for the first len[i] records with key >= start[i]; a
+// locate pass descends and computes each query's count, an exclusive scan
+// turns counts into offsets, and a copy pass (one warp per query) writes the
+// records contiguously: leaves are ordered, so the records of a query are the
+// key-ordered run that starts at (leaf, slot) and continues in leaf+1, ...
+#include "hm_internal.cuh"
+
+namespace hm {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+int scan_ctas(int64_t n) {
+  int64_t c = (n + 4095) / 4096;
+  if (c > 148 * 4) c = 148 * 4;
+  if (c < 1) c = 1;
+  return (int)c;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) seg_sum_kernel(const T *__restrict__ in, int64_t n,
+                                                           int64_t seg, int64_t *__restrict__ part) {
+  __shared__ int64_t red[kThreads / 32];
+  int64_t b0 = (int64_t)blockIdx.x * seg, b1 = min(n, b0 + seg);
+  int64_t s = 0;
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += kThreads) s += (int64_t)in[i];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t t = 0;
+    for (int w = 0; w < kThreads / 32; w++) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+// Exclusive scan of each segment, offset by the scanned segment sums.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) seg_scan_kernel(const T *__restrict__ in, int64_t n,
+                                                            int64_t seg, const int64_t *__restrict__ part,
+                                                            int64_t *__restrict__ out, int nctas) {
+  __shared__ int64_t wsum[kThreads / 32];
+  __shared__ int64_t carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t b0 = (int64_t)blockIdx.x * seg, b1 = min(n, b0 + seg);
+  if (threadIdx.x == 0) carry = part[blockIdx.x];
+  __syncthreads();
+  for (int64_t t0 = b0; t0 < b1; t0 += kThreads) {
+    int64_t i = t0 + threadIdx.x;
+    int64_t v = i < b1 ? (int64_t)in[i] : 0;
+    int64_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    int64_t before = carry;
+    for (int w = 0; w < warp; w++) before += wsum[w];
+    if (i < b1) out[i] = before + x - v;
+    __syncthreads();
+    if (threadIdx.x == kThreads - 1) carry = before + x;
+    __syncthreads();
+  }
+  if (blockIdx.x == nctas - 1 && threadIdx.x == 0) out[n] = carry;
+}
+
+__global__ void export_kernel(DevTree t, int lc, int li, int64_t *__restrict__ keys,
+                              int64_t *__restrict__ vals) {
+  const int64_t total = (int64_t)t.n_leaf * lc;
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    int64_t j = x / lc;
+    int s = (int)(x - j * lc);
+    if (s < t.leaf_cnt[j]) {
+      int64_t o = t.leaf_base[j] + s;
+      keys[o] = t.leaf_keys[j * (li + lc) + li + s];
+      vals[o] = t.leaf_vals[j * lc + s];
+    }
+  }
+}
+
+// Scalar descent to the leaf holding the position of q (one thread).
+__device__ __forceinline__ int32_t descend_scalar(const DevTree &t, int f, int64_t q) {
+  const int ix = f / 8, row = ix + f;
+  int32_t node = 0;
+  for (int l = 0; l < t.height; l++) {
+    const int64_t *r = t.inner + (int64_t)node * row;
+    int k = 0;
+    for (int v = 0; v < ix / 2; v++) {
+      longlong2 p = __ldg(reinterpret_cast<const longlong2 *>(r + 2 * v));
+      k += (p.x <= q) + (p.y <= q);
+    }
+    k = min(k, ix - 1);
+    int c = 8 * k;
+    for (int v = 0; v < 4; v++) {
+      longlong2 p = __ldg(reinterpret_cast<const longlong2 *>(r + ix + 8 * k + 2 * v));
+      c += (p.x <= q) + (p.y <= q);
+    }
+    node = __ldg(t.prefix + node) + c;
+  }
+  return node - t.n_inner;
+}
+
+__global__ void range_locate_kernel(DevTree t, int f, int lc, int li, const int64_t *__restrict__ start,
+                                    const int32_t *__restrict__ len, int64_t n,
+                                    int32_t *__restrict__ first_leaf, int32_t *__restrict__ first_slot,
+                                    int64_t *__restrict__ count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t s = __ldg(start + i);
+    int64_t want = __ldg(len + i);
+    if (want <= 0 || s == kMaxKey || t.n_keys == 0) {
+      first_leaf[i] = 0;
+      first_slot[i] = 0;
+      count[i] = 0;
+      continue;
+    }
+    int32_t leaf = descend_scalar(t, f, s);
+    const int64_t *kr = t.leaf_keys + (int64_t)leaf * (li + lc) + li;
+    int cnt = __ldg(t.leaf_cnt + leaf);
+    int lb = 0;  // first slot with key >= start
+    while (lb < cnt && __ldg(kr + lb) < s) lb++;
+    int64_t g = __ldg(t.leaf_base + leaf) + lb;
+    int64_t rem = t.n_keys - g;
+    first_leaf[i] = leaf;
+    first_slot[i] = lb;
+    count[i] = want < rem ? want : rem;
+  }
+}
+
+__global__ void range_copy_kernel(DevTree t, int lc, int li, const int32_t *__restrict__ first_leaf,
+                                  const int32_t *__restrict__ first_slot,
+                                  const int64_t *__restrict__ offsets, int64_t n,
+                                  int64_t *__restrict__ okeys, int64_t *__restrict__ ovals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + (threadIdx.x >> 5); i < n; i += warps) {
+    int64_t o = offsets[i];
+    int64_t rem = offsets[i + 1] - o;
+    int32_t leaf = first_leaf[i];
+    int slot = first_slot[i];
+    while (rem > 0 && leaf < t.n_leaf) {
+      int avail = __ldg(t.leaf_cnt + leaf) - slot;
+      int take = (int)(avail < rem ? avail : rem);
+      const int64_t *kr = t.leaf_keys + (int64_t)leaf * (li + lc) + li + slot;
+      const int64_t *vr = t.leaf_vals + (int64_t)leaf * lc + slot;
+      for (int x = lane; x < take; x += 32) {
+        okeys[o + x] = __ldg(kr + x);
+        ovals[o + x] = __ldg(vr + x);
+      }
+      o += take;
+      rem -= take;
+      leaf++;
+      slot = 0;
+    }
+  }
+}
+
+unsigned grid_for_items(int64_t items, unsigned cap) {
+  int64_t b = (items + kThreads - 1) / kThreads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (unsigned)b;
+}
+
+}  // namespace
+
+size_t scan_scratch_bytes(int64_t n) { return sizeof(int64_t) * (scan_ctas(n) + 8); }
+
+template <typename T>
+void exclusive_scan(const T *in, int64_t *out, int64_t n, void *scratch, cudaStream_t s) {
+  const int nctas = scan_ctas(n);
+  const int64_t seg = (n + nctas - 1) / nctas;
+  int64_t *part = static_cast<int64_t *>(scratch);
+  if (n == 0) {
+    cudaMemsetAsync(out, 0, sizeof(int64_t), s);
+    return;
+  }
+  seg_sum_kernel<T><<<nctas, kThreads, 0, s>>>(in, n, seg, part);
+  scan_counts(part, nctas, s);
+  seg_scan_kernel<T><<<nctas, kThreads, 0, s>>>(in, n, seg, part, out, nctas);
+  note_launch(2);
+}
+
+void scan_counts(int64_t *counts, int64_t m, cudaStream_t s);
+
+void exclusive_scan_i64(const int64_t *in, int64_t *out, int64_t n, void *scratch, cudaStream_t s) {
+  exclusive_scan<int64_t>(in, out, n, scratch, s);
+}
+
+void exclusive_scan_i32(const int32_t *in, int64_t *out, int64_t n, void *scratch, cudaStream_t s) {
+  exclusive_scan<int32_t>(in, out, n, scratch, s);
+}
+
+void export_contents(const hm_tree *t, int64_t *d_keys, int64_t *d_vals, cudaStream_t s) {
+  if (t->n_keys == 0) return;
+  export_kernel<<<grid_for_items(t->n_leaf * t->cfg.leaf_cap, 148u * 32), kThreads, 0, s>>>(
+      t->view(), t->cfg.leaf_cap, t->leaf_index, d_keys, d_vals);
+  note_launch();
+}
+
+size_t range_scratch_bytes(int64_t n) {
+  return (size_t)align_up(n * 4, 256) * 2 + (size_t)align_up(n * 8, 256) + scan_scratch_bytes(n) + 256;
+}
+
+int range_locate(const hm_tree *t, const int64_t *start, const int32_t *len, int64_t n,
+                 int32_t *first_leaf, int32_t *first_slot, int64_t *count, cudaStream_t s) {
+  range_locate_kernel<<<grid_for_items(n, 148u * 16), kThreads, 0, s>>>(
+      t->view(), t->cfg.fanout, t->cfg.leaf_cap, t->leaf_index, start, len, n, first_leaf,
+      first_slot, count);
+  note_launch();
+  return cuda_err(cudaGetLastError());
+}
+
+int range_copy_out(const hm_tree *t, const int32_t *first_leaf, const int32_t *first_slot,
+                   const int64_t *offsets, int64_t n, int64_t *okeys, int64_t *ovals, cudaStream_t s) {
+  int64_t warps = n;
+  int64_t blocks = (warps + (kThreads / 32) - 1) / (kThreads / 32);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  range_copy_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(t->view(), t->cfg.leaf_cap, t->leaf_index,
+                                                         first_leaf, first_slot, offsets, n, okeys,
+                                                         ovals);
+  note_launch();
+  return cuda_err(cudaGetLastError());
+}
+
+}  // namespace hm

@@ -1,0 +1,395 @@
+// One epoch of batched upserts applied on the GPU.
+//
+// Reference: BPlusTree::insert_parallel_Newupdate_batch
+// (open-harmonia/src/bpt-ppi-update-batch.cpp:86-200): 56 CPU threads
+// descend per key, update an existing key under the leaf mutex
+// (value = key-1, :47) or insert into the record list if it has room
+// (:59-67), a leaf inner split otherwise (:71-76), a serial insert for the
+// rest (:151-170) and a periodic re-BFS of the inner nodes
+// (rebuild_without_leaf, open-harmonia/src/bpt-ppi-update.cpp:320-463).  The
+// reference never refreshes the GPU copy.
+//
+// Here the epoch runs on the device tree itself:
+//   1. sort the batch by key (stable, payload = input index) and keep the
+//      last occurrence of each key;
+//   2. one thread per key descends; a hit overwrites the value in place
+//      (supplied value, or key-1 under HM_UPSERT_REF_KEY_MINUS_1);
+//   3. the misses, still in key order, are grouped by leaf; if every touched
+//      leaf has room, one warp per leaf merges its new keys into the sorted
+//      row (separators stay valid: a key routed to leaf j lies in
+//      [separator_j, separator_j+1)), and leaf_base is rescanned;
+//   4. otherwise the tree is rebuilt: the current contents and the misses
+//      are merged (each element's output slot = own rank + rank in the other
+//      run) and bulk-loaded into a fresh arena with the same parameters.
+#include "hm_internal.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace hm {
+
+void scan_counts(int64_t *counts, int64_t m, cudaStream_t s);
+void exclusive_scan_i32(const int32_t *in, int64_t *out, int64_t n, void *scratch, cudaStream_t s);
+void export_contents(const hm_tree *t, int64_t *d_keys, int64_t *d_vals, cudaStream_t s);
+
+namespace {
+
+constexpr int kThreads = 256;
+
+unsigned grid_for(int64_t items) {
+  int64_t b = (items + kThreads - 1) / kThreads;
+  if (b < 1) b = 1;
+  if (b > 148 * 16) b = 148 * 16;
+  return (unsigned)b;
+}
+
+__global__ void iota_kernel(int64_t *p, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = i;
+}
+
+// keep[i] = 1 for the last occurrence of each key in the sorted batch;
+// flags bit1 if a key equals Max_Key.
+__global__ void last_occurrence_kernel(const uint64_t *__restrict__ uk, int64_t n,
+                                       int32_t *__restrict__ keep, unsigned *flags) {
+  unsigned f = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    keep[i] = (i == n - 1 || uk[i] != uk[i + 1]) ? 1 : 0;
+    if ((int64_t)(uk[i] ^ kSign) == kMaxKey) f |= 2u;
+  }
+  if (f) atomicOr(flags, f);
+}
+
+__global__ void compact_batch_kernel(const uint64_t *__restrict__ uk, const int64_t *__restrict__ idx,
+                                     const int64_t *__restrict__ vals, const int32_t *__restrict__ keep,
+                                     const int64_t *__restrict__ at, int64_t n,
+                                     int64_t *__restrict__ bk, int64_t *__restrict__ bv) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (keep[i]) {
+      int64_t o = at[i];
+      bk[o] = (int64_t)(uk[i] ^ kSign);
+      bv[o] = vals[idx[i]];
+    }
+  }
+}
+
+__device__ __forceinline__ int32_t descend_to_leaf(const DevTree &t, int f, int64_t q) {
+  const int ix = f / 8, row = ix + f;
+  int32_t node = 0;
+  for (int l = 0; l < t.height; l++) {
+    const int64_t *r = t.inner + (int64_t)node * row;
+    int k = 0;
+    for (int v = 0; v < ix; v++) k += (r[v] <= q);
+    k = min(k, ix - 1);
+    int c = 8 * k;
+    for (int v = 0; v < 8; v++) c += (r[ix + 8 * k + v] <= q);
+    node = t.prefix[node] + c;
+  }
+  return node - t.n_inner;
+}
+
+// Hits are updated in place; misses get miss[i] = 1 and their leaf.
+__global__ void apply_kernel(DevTree t, int f, int lc, int li, int flags,
+                             const int64_t *__restrict__ bk, const int64_t *__restrict__ bv, int64_t m,
+                             int64_t *leaf_vals, int32_t *__restrict__ miss,
+                             int32_t *__restrict__ leaf_of) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t k = bk[i];
+    int32_t leaf = descend_to_leaf(t, f, k);
+    const int64_t *kr = t.leaf_keys + (int64_t)leaf * (li + lc) + li;
+    int cnt = t.leaf_cnt[leaf];
+    int slot = -1;
+    for (int s = 0; s < cnt; s++)
+      if (kr[s] == k) slot = s;
+    leaf_of[i] = leaf;
+    if (slot >= 0) {
+      leaf_vals[(int64_t)leaf * lc + slot] = (flags & HM_UPSERT_REF_KEY_MINUS_1) ? k - 1 : bv[i];
+      miss[i] = 0;
+    } else {
+      miss[i] = 1;
+    }
+  }
+}
+
+__global__ void compact_miss_kernel(const int64_t *__restrict__ bk, const int64_t *__restrict__ bv,
+                                    const int32_t *__restrict__ leaf_of, const int32_t *__restrict__ miss,
+                                    const int64_t *__restrict__ at, int64_t m, int64_t *__restrict__ mk,
+                                    int64_t *__restrict__ mv, int32_t *__restrict__ ml) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (miss[i]) {
+      int64_t o = at[i];
+      mk[o] = bk[i];
+      mv[o] = bv[i];
+      ml[o] = leaf_of[i];
+    }
+  }
+}
+
+// For each run of misses on one leaf (misses are in key order, so leaves are
+// non-decreasing): seg_start[leaf] = first miss index, add[leaf] = run length;
+// flags bit0 if the leaf would overflow.
+__global__ void miss_runs_kernel(const int32_t *__restrict__ ml, int64_t nm,
+                                 const int32_t *__restrict__ leaf_cnt, int lc,
+                                 int64_t *__restrict__ run_start, int32_t *__restrict__ run_len,
+                                 int32_t *__restrict__ run_leaf, int32_t *__restrict__ is_start,
+                                 unsigned *flags) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    bool st = (i == 0) || ml[i] != ml[i - 1];
+    is_start[i] = st ? 1 : 0;
+    if (st) {
+      int64_t e = i + 1;
+      while (e < nm && ml[e] == ml[i]) e++;
+      run_start[i] = i;
+      run_len[i] = (int32_t)(e - i);
+      run_leaf[i] = ml[i];
+      if (leaf_cnt[ml[i]] + (e - i) > lc) atomicOr(flags, 1u);
+    }
+  }
+}
+
+// One warp per run: merge the run's new keys into the leaf row.
+__global__ void merge_leaf_kernel(int64_t *leaf_keys, int64_t *leaf_vals, int32_t *leaf_cnt, int lc,
+                                  int li, const int64_t *__restrict__ mk, const int64_t *__restrict__ mv,
+                                  const int32_t *__restrict__ is_start,
+                                  const int64_t *__restrict__ run_start,
+                                  const int32_t *__restrict__ run_len,
+                                  const int32_t *__restrict__ run_leaf, int64_t nm) {
+  __shared__ int64_t sk[kThreads / 32][128];
+  __shared__ int64_t sv[kThreads / 32][128];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + w; i < nm; i += warps) {
+    if (!is_start[i]) continue;
+    const int32_t leaf = run_leaf[i];
+    const int64_t r0 = run_start[i];
+    const int rl = run_len[i];
+    int64_t *kr = leaf_keys + (int64_t)leaf * (li + lc) + li;
+    int64_t *vr = leaf_vals + (int64_t)leaf * lc;
+    const int cnt = leaf_cnt[leaf];
+    // existing key a goes to a + #(new < key); new key b to b + #(existing < key)
+    for (int a = lane; a < cnt; a += 32) {
+      int64_t k = kr[a];
+      int below = 0;
+      for (int b = 0; b < rl; b++) below += (mk[r0 + b] < k);
+      sk[w][a + below] = k;
+      sv[w][a + below] = vr[a];
+    }
+    for (int b = lane; b < rl; b += 32) {
+      int64_t k = mk[r0 + b];
+      int below = 0;
+      for (int a = 0; a < cnt; a++) below += (kr[a] < k);
+      sk[w][b + below] = k;
+      sv[w][b + below] = mv[r0 + b];
+    }
+    __syncwarp();
+    const int nc = cnt + rl;
+    for (int x = lane; x < lc; x += 32) {
+      kr[x] = x < nc ? sk[w][x] : kMaxKey;
+      vr[x] = x < nc ? sv[w][x] : (int64_t)HM_NOT_FOUND;
+    }
+    __syncwarp();
+    if (li > 0) {
+      int64_t *ir = leaf_keys + (int64_t)leaf * (li + lc);
+      for (int x = lane; x < li; x += 32) ir[x] = (8 * (x + 1) < lc) ? kr[8 * (x + 1)] : kMaxKey;
+    }
+    if (lane == 0) leaf_cnt[leaf] = nc;
+    __syncwarp();
+  }
+}
+
+// Merge of two sorted, disjoint runs: out slot = own index + rank in the other run.
+__global__ void merge_rank_kernel(const int64_t *__restrict__ a, const int64_t *__restrict__ av, int64_t na,
+                                  const int64_t *__restrict__ b, int64_t nb, bool strict,
+                                  uint64_t *__restrict__ ok, int64_t *__restrict__ ov) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < na;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t k = a[i];
+    int64_t lo = 0, hi = nb;  // first b >= k (strict) or > k
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      bool before = strict ? (b[mid] < k) : (b[mid] <= k);
+      if (before) lo = mid + 1; else hi = mid;
+    }
+    ok[i + lo] = (uint64_t)k ^ kSign;
+    ov[i + lo] = av[i];
+  }
+}
+
+size_t al(int64_t bytes) { return (size_t)align_up(bytes, 256); }
+
+}  // namespace
+
+int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64_t n, int flags,
+                 cudaStream_t s) {
+  if (n <= 0) return HM_OK;
+  const int lc = t->cfg.leaf_cap, li = t->leaf_index, f = t->cfg.fanout;
+  // scratch: uk, uk_alt, idx, idx_alt (n each, 8 B), keep/miss/leaf_of/is_start (4 B),
+  // at (8 B, n+1), bk, bv, mk, mv, run_start (8 B), run_len/run_leaf/ml (4 B), sort scratch, flags
+  const size_t s8 = al(8 * (n + 1)), s4 = al(4 * (n + 1));
+  size_t need = 9 * s8 + 7 * s4 + al((int64_t)radix_scratch_bytes(n)) + al((int64_t)scan_scratch_bytes(n + 1)) + 256;
+  int rc = ensure_scratch(t, need);
+  if (rc) return rc;
+  char *p = static_cast<char *>(t->scratch);
+  auto take8 = [&](void) { char *r = p; p += s8; return r; };
+  auto take4 = [&](void) { char *r = p; p += s4; return r; };
+  uint64_t *uk = reinterpret_cast<uint64_t *>(take8());
+  uint64_t *uk_alt = reinterpret_cast<uint64_t *>(take8());
+  int64_t *idx = reinterpret_cast<int64_t *>(take8());
+  int64_t *idx_alt = reinterpret_cast<int64_t *>(take8());
+  int64_t *at = reinterpret_cast<int64_t *>(take8());
+  int64_t *bk = reinterpret_cast<int64_t *>(take8());
+  int64_t *bv = reinterpret_cast<int64_t *>(take8());
+  int64_t *mk = reinterpret_cast<int64_t *>(take8());
+  int64_t *mv = reinterpret_cast<int64_t *>(take8());
+  int32_t *keep = reinterpret_cast<int32_t *>(take4());
+  int32_t *miss = reinterpret_cast<int32_t *>(take4());
+  int32_t *leaf_of = reinterpret_cast<int32_t *>(take4());
+  int32_t *ml = reinterpret_cast<int32_t *>(take4());
+  int32_t *is_start = reinterpret_cast<int32_t *>(take4());
+  int32_t *run_len = reinterpret_cast<int32_t *>(take4());
+  int32_t *run_leaf = reinterpret_cast<int32_t *>(take4());
+  int64_t *run_start = idx_alt;  // free once the sort is done
+  void *sort_scratch = p;
+  p += al((int64_t)radix_scratch_bytes(n));
+  void *scan_scratch = p;
+  p += al((int64_t)scan_scratch_bytes(n + 1));
+  unsigned *dflags = reinterpret_cast<unsigned *>(p);
+
+  cudaMemsetAsync(dflags, 0, 8, s);
+  transform_keys_in(d_keys, uk, n, s);
+  iota_kernel<<<grid_for(n), kThreads, 0, s>>>(idx, n);
+  note_launch();
+  if (radix_sort_pairs<int64_t>(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) {
+    std::swap(uk, uk_alt);
+    std::swap(idx, idx_alt);
+  }
+  run_start = idx_alt;
+  last_occurrence_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, n, keep, dflags);
+  exclusive_scan_i32(keep, at, n, scan_scratch, s);
+  compact_batch_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, idx, d_vals, keep, at, n, bk, bv);
+  note_launch(2);
+  int64_t hm_[2] = {0, 0};
+  unsigned hf = 0;
+  cudaMemcpyAsync(&hm_[0], at + n, 8, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&hf, dflags, 4, cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_err(e);
+  if (hf & 2u) return HM_EMAXKEY;
+  const int64_t m = hm_[0];
+
+  apply_kernel<<<grid_for(m), kThreads, 0, s>>>(t->view(), f, lc, li, flags, bk, bv, m, t->leaf_vals,
+                                                miss, leaf_of);
+  exclusive_scan_i32(miss, at, m, scan_scratch, s);
+  compact_miss_kernel<<<grid_for(m), kThreads, 0, s>>>(bk, bv, leaf_of, miss, at, m, mk, mv, ml);
+  note_launch(2);
+  cudaMemcpyAsync(&hm_[1], at + m, 8, cudaMemcpyDeviceToHost, s);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_err(e);
+  const int64_t nm = hm_[1];
+  if (nm == 0) return HM_OK;
+
+  cudaMemsetAsync(dflags, 0, 4, s);
+  miss_runs_kernel<<<grid_for(nm), kThreads, 0, s>>>(ml, nm, t->leaf_cnt, lc, run_start, run_len,
+                                                      run_leaf, is_start, dflags);
+  note_launch();
+  cudaMemcpyAsync(&hf, dflags, 4, cudaMemcpyDeviceToHost, s);
+  int64_t new_ends[2];
+  cudaMemcpyAsync(&new_ends[0], mk, 8, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&new_ends[1], mk + nm - 1, 8, cudaMemcpyDeviceToHost, s);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_err(e);
+
+  if (!(hf & 1u)) {
+    // Every touched leaf has room: merge in place.
+    int64_t blocks = (nm + 7) / 8;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    merge_leaf_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(t->leaf_keys, t->leaf_vals, t->leaf_cnt, lc,
+                                                            li, mk, mv, is_start, run_start, run_len,
+                                                            run_leaf, nm);
+    exclusive_scan_i32(t->leaf_cnt, at, t->n_leaf, scan_scratch, s);
+    cudaMemcpyAsync(t->leaf_base, at, 8 * t->n_leaf, cudaMemcpyDeviceToDevice, s);
+    note_launch();
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_err(e);
+    t->n_keys += nm;
+  } else {
+    // Rebuild: contents (already carrying this epoch's in-place updates)
+    // merged with the misses, then a bulk load into a fresh arena.
+    const int64_t n0 = t->n_keys, n1 = n0 + nm;
+    int64_t *ek = nullptr, *ev = nullptr;
+    uint64_t *ck = nullptr;
+    int64_t *cv = nullptr, *tmp_a = nullptr, *tmp_b = nullptr;
+    hm_tree nt = *t;  // new shape in a copy; arena swapped in at the end
+    nt.scratch = nullptr;
+    rc = shape(n1, t->cfg, &nt.height, nt.lvl_start, &nt.n_inner, &nt.n_leaf);
+    if (rc) return rc;
+    size_t off_prefix = al(nt.n_inner * nt.inner_row * 8);
+    size_t off_lkeys = off_prefix + al(align_up(nt.n_inner, 4) * 4);
+    size_t off_lvals = off_lkeys + al(nt.n_leaf * nt.leaf_row * 8);
+    size_t off_lcnt = off_lvals + al(nt.n_leaf * lc * 8);
+    size_t off_lbase = off_lcnt + al(nt.n_leaf * 4);
+    size_t total = off_lbase + al(nt.n_leaf * 8);
+    int64_t tn = std::max<int64_t>(std::max<int64_t>(n1, nt.n_leaf), 1);
+    char *tmp = nullptr;
+    e = cudaMalloc(&nt.arena, total);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, 6 * al(8 * tn));
+    if (e != cudaSuccess) {
+      if (nt.arena) cudaFree(nt.arena);
+      if (tmp) cudaFree(tmp);
+      return cuda_err(e);
+    }
+    ek = reinterpret_cast<int64_t *>(tmp);
+    ev = reinterpret_cast<int64_t *>(tmp + al(8 * tn));
+    ck = reinterpret_cast<uint64_t *>(tmp + 2 * al(8 * tn));
+    cv = reinterpret_cast<int64_t *>(tmp + 3 * al(8 * tn));
+    tmp_a = reinterpret_cast<int64_t *>(tmp + 4 * al(8 * tn));
+    tmp_b = reinterpret_cast<int64_t *>(tmp + 5 * al(8 * tn));
+    export_contents(t, ek, ev, s);
+    merge_rank_kernel<<<grid_for(n0), kThreads, 0, s>>>(ek, ev, n0, mk, nm, true, ck, cv);
+    merge_rank_kernel<<<grid_for(nm), kThreads, 0, s>>>(mk, mv, nm, ek, n0, true, ck, cv);
+    note_launch(2);
+    char *base = static_cast<char *>(nt.arena);
+    cudaMemsetAsync(base, 0, total, s);
+    nt.arena_bytes = total;
+    nt.inner = reinterpret_cast<int64_t *>(base);
+    nt.prefix = reinterpret_cast<int32_t *>(base + off_prefix);
+    nt.leaf_keys = reinterpret_cast<int64_t *>(base + off_lkeys);
+    nt.leaf_vals = reinterpret_cast<int64_t *>(base + off_lvals);
+    nt.leaf_cnt = reinterpret_cast<int32_t *>(base + off_lcnt);
+    nt.leaf_base = reinterpret_cast<int64_t *>(base + off_lbase);
+    nt.n_keys = n1;
+    rc = build_from_sorted(&nt, ck, cv, n1, tmp_a, tmp_b, s);
+    e = cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
+    if (rc) {
+      cudaFree(nt.arena);
+      return rc;
+    }
+    cudaFree(t->arena);
+    t->arena = nt.arena;
+    t->arena_bytes = nt.arena_bytes;
+    t->inner = nt.inner;
+    t->prefix = nt.prefix;
+    t->leaf_keys = nt.leaf_keys;
+    t->leaf_vals = nt.leaf_vals;
+    t->leaf_cnt = nt.leaf_cnt;
+    t->leaf_base = nt.leaf_base;
+    t->height = nt.height;
+    std::memcpy(t->lvl_start, nt.lvl_start, sizeof(t->lvl_start));
+    t->n_inner = nt.n_inner;
+    t->n_leaf = nt.n_leaf;
+    t->n_keys = n1;
+  }
+  if (t->n_keys == nm || new_ends[0] < t->key_min) t->key_min = new_ends[0];
+  if (t->n_keys == nm || new_ends[1] > t->key_max) t->key_max = new_ends[1];
+  return HM_OK;
+}
+
+}  // namespace hm

@@ -1,0 +1,205 @@
+/* harmonia-b200: batched B+tree search, range scan and batched upsert on one
+ * NVIDIA B200 (sm_100a), behind a C ABI.
+ *
+ * The reference (fudan-ppi/harmonia, open-harmonia/) has no library API: each
+ * experiment is `void fn(BPlusTree &tree, std::ifstream &search_file)`
+ * (open-harmonia/src/ppi-bpt.h:4-98, open-harmonia/regular_bpt/gpu-cfb.h:2-8)
+ * that builds, uploads, searches and frees inside one call, and errors end
+ * the process (open-harmonia/src/cuda_utils.h:3-12).  The entry points below
+ * replace those calls one to one; each names the reference code it stands in
+ * for.  All functions return HM_OK (0) or a negative HM_E* code; none exits.
+ *
+ * Keys and values are int64 compared as signed integers.  INT64_MAX is the
+ * empty-slot sentinel (Max_Key, open-harmonia/src/bpt.h:26) and cannot be
+ * stored; a search for it returns "not found".  Not found is -1
+ * (open-harmonia/src/bpt.h:272).
+ *
+ * Pointers passed as query/result buffers may be host or device memory
+ * (detected per call).  With device buffers a call only enqueues work on the
+ * given stream and returns; with host buffers it copies in chunks through
+ * pinned staging, overlapping copies with the search, and returns when the
+ * results are in host memory.  Calls on one tree are serialised by the caller;
+ * read-only calls (search, range) may run concurrently on different streams.
+ */
+#ifndef HARMONIA_H
+#define HARMONIA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default) /* the library builds with -fvisibility=hidden */
+#endif
+
+#define HM_MAX_KEY INT64_MAX
+#define HM_NOT_FOUND (-1)
+
+enum {
+  HM_OK = 0,
+  HM_EINVAL = -1,      /* bad argument or configuration */
+  HM_ENOMEM = -2,      /* device or pinned-host allocation failed */
+  HM_EDUPLICATE = -3,  /* bulk load: a key occurs twice */
+  HM_EMAXKEY = -4,     /* a key equals the sentinel INT64_MAX */
+  HM_ECUDA = -5,       /* a CUDA runtime call failed */
+  HM_ECAPACITY = -6,   /* range: output capacity too small */
+  HM_ETIMEOUT = -7,    /* a bounded device-side wait gave up */
+  HM_ENODEVICE = -8,   /* no usable CUDA device */
+  HM_EBUSY = -9,       /* serving: queue full or budget exhausted */
+  HM_ECANCELLED = -10, /* serving: request cancelled or server stopped */
+  HM_ETOOLARGE = -11   /* a size exceeds a documented maximum */
+};
+
+typedef void *hm_stream; /* a cudaStream_t; NULL = the legacy default stream */
+typedef struct hm_tree hm_tree;
+
+/* Layout and search parameters.  The reference fixes these at compile time:
+ * BPT_ORDER 64 (open-harmonia/src/bpt.h:15), DEFAULT_ORDER / Narrow_Rate from
+ * CMake (open-harmonia/CMakeLists.txt:55-57), Thread_Per_Query and
+ * GPU_SWP_SIZE per file (open-harmonia/src/full-multi-prefix-sort-8thread.cu:19-29),
+ * sort bits [48,64) (same file :305-309).  Zero means "default" everywhere. */
+typedef struct {
+  int fanout;            /* inner-node key slots: 64 or 128 (default 64) */
+  int leaf_cap;          /* leaf key slots: 16 or 64 (default 16) */
+  int inner_fill;        /* children per inner node at bulk load, 2..fanout (default fanout) */
+  int leaf_fill;         /* keys per leaf at bulk load, 1..leaf_cap (default leaf_cap) */
+  int group_width;       /* lanes cooperating on one query: 1,2,4,8,16,32 (default 4) */
+  int queries_per_group; /* queries a group keeps in flight: 1,2,4 (default 2) */
+  int sort_bits;         /* query pre-sort: top bits partitioned, 0 = off, -1 = auto (default -1) */
+  int smem_bytes;        /* budget for top levels staged in shared memory (default 49152) */
+  int cache_hints;       /* L2 policy: 1 = inner rows evict_last, leaves evict_first; 2 = none
+                            (default 1) */
+} hm_config;
+
+/* Read-only description of a loaded tree. */
+typedef struct {
+  int fanout, leaf_cap, height; /* height = number of inner levels */
+  int inner_row_words;          /* int64 words per inner row: fanout/8 index + fanout keys */
+  int leaf_row_words;           /* int64 words per leaf key row */
+  int leaf_index_words;         /* index words at the start of a leaf row (leaf_cap >= 32) */
+  int smem_levels;              /* top levels staged in shared memory by the search kernel */
+  int64_t n_keys, n_inner, n_leaf;
+  int64_t lvl_start[33];        /* BFS id of each inner level's first node */
+  /* device pointers into the tree's HBM arena */
+  const int64_t *inner;     /* n_inner rows */
+  const int32_t *prefix;    /* n_inner first-child ids (leaves count from n_inner) */
+  const int64_t *leaf_keys; /* n_leaf rows */
+  const int64_t *leaf_vals; /* n_leaf * leaf_cap */
+  const int32_t *leaf_cnt;  /* n_leaf */
+  const int64_t *leaf_base; /* n_leaf, exclusive scan of leaf_cnt */
+  size_t device_bytes;      /* bytes of the tree arena */
+} hm_tree_info;
+
+/* Fills *cfg with the defaults. */
+int hm_config_default(hm_config *cfg);
+
+/* Builds a device-resident tree from n (key, value) pairs on the GPU: sort,
+ * duplicate/sentinel check, leaves, then inner levels with the prefix-sum
+ * child array.  Keys need not be sorted.
+ * Replaces: the serial BPlusTree::insert loop + BPlusTree::sort + the upload
+ * (open-harmonia/src/main.cpp:50-67,151-152; open-harmonia/src/traversal.cpp:35-195;
+ * prepareGPU_v2 / prepareGPU_leaf, open-harmonia/src/prepareGPU.cu:140-163;
+ * CFB generateCFB + prepareGPU, open-harmonia/regular_bpt/traversal.cpp:81-99,
+ * open-harmonia/regular_bpt/helper.cu:12-28). */
+int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n,
+                 const hm_config *cfg, hm_tree **out);
+
+/* Batched point search: out[i] = value of q[i], or -1.
+ * Replaces: full_multi_prefix_sort_8thread (+ its kernel and the CUB
+ * pre-sort), open-harmonia/src/full-multi-prefix-sort-8thread.cu:95-495, and
+ * multi_prefix_sort, open-harmonia/regular_bpt/prefix-sort.cu:98-478; the
+ * result decode of the same file :454-476 is done on the device. */
+int hm_search(hm_tree *t, const int64_t *q, size_t n, int64_t *out, hm_stream s);
+
+/* One query batch of a multi-batch launch. */
+typedef struct {
+  const int64_t *q; /* device pointer */
+  int64_t *out;     /* device pointer */
+  int64_t n;
+} hm_batch;
+
+/* Searches nb independent batches (device buffers) in one persistent kernel.
+ * Replaces: the per-bucket launch loop of launch_kernel_thread,
+ * open-harmonia/src/full-multi-prefix-sort-8thread.cu:276-327. */
+int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream s);
+
+/* Range scan: for query i the first len[i] records with key >= start[i], in
+ * key order (fewer if the key space ends), compacted: query i's records are
+ * okeys/ovals[offsets[i] .. offsets[i+1]).  offsets has n+1 entries; *total
+ * receives offsets[n].  Returns HM_ECAPACITY (with *total set) when cap is
+ * too small.
+ * Replaces: range_prefix_sort_1thread_search_and_1thread_scan and its kernel,
+ * open-harmonia/src/range.cu:101-227,312-360 (fixed Range_Size=8 slots, end
+ * key forced to Max_Key), and traverse_PPItree, open-harmonia/src/cpu-range.cpp:129-183. */
+int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n,
+             int64_t *offsets, int64_t *okeys, int64_t *ovals, size_t cap,
+             size_t *total, hm_stream s);
+
+#define HM_UPSERT_SUPPLIED 0        /* an existing key takes the supplied value */
+#define HM_UPSERT_REF_KEY_MINUS_1 1 /* an existing key takes key-1, as the reference does */
+
+/* Applies one epoch of upserts on the GPU: existing keys are updated in
+ * place, new keys are merged into their leaves, and leaves that overflow
+ * trigger a rebuild.  Within one batch the last occurrence of a key wins.
+ * Replaces: BPlusTree::insert_parallel_Newupdate_batch and its worker
+ * (open-harmonia/src/bpt-ppi-update-batch.cpp:10-200), insert_Newupdate and
+ * rebuild_without_leaf (open-harmonia/src/bpt-ppi-update.cpp:99-138,320-463). */
+int hm_upsert_batch(hm_tree *t, const int64_t *keys, const int64_t *vals,
+                    size_t n, int flags, hm_stream s);
+
+/* Sorted contents of the tree into host or device buffers; *n receives the
+ * key count.  Returns HM_ECAPACITY if cap < count.
+ * Replaces: the ENABLE_TEST decode/print loops of the reference drivers
+ * (open-harmonia/src/full-multi-prefix-sort-8thread.cu:454-476). */
+int hm_export(hm_tree *t, int64_t *keys, int64_t *vals, size_t cap, size_t *n);
+
+int hm_tree_get_info(const hm_tree *t, hm_tree_info *info);
+
+/* Changes the search parameters of a loaded tree (group_width,
+ * queries_per_group, sort_bits, smem_bytes); layout fields are ignored. */
+int hm_set_search_config(hm_tree *t, const hm_config *cfg);
+int hm_get_config(const hm_tree *t, hm_config *cfg);
+
+/* Times candidate search parameters on a sample of queries (device buffer)
+ * and keeps the fastest: group width {2,4,8,16,32} x queries per group
+ * x sort bits.  Writes the chosen config to *best (may be NULL).
+ * Replaces: the recompile-per-point sweeps open-harmonia/tests/multi-regular-narrow.sh
+ * and open-harmonia/tests/bit-prefix-sort-8thread.sh. */
+int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n, hm_config *best);
+
+/* Waits for the tree's outstanding work on stream s and returns any error a
+ * kernel recorded (HM_ETIMEOUT for a bounded wait that gave up). */
+int hm_sync(hm_tree *t, hm_stream s);
+
+int hm_free(hm_tree *t);
+const char *hm_strerror(int code);
+
+/* Kernel launches this library has issued since load (for launch counting). */
+uint64_t hm_launch_count(void);
+
+/* Per-stage device time, measured with CUDA events recorded on the stream
+ * each stage's kernels run on.  Stages: "partition" (query pre-sort),
+ * "search" (descent + leaf test), "search_batches", "range", "upsert".
+ * Replaces: the cudaEvent timing of the reference drivers
+ * (open-harmonia/src/full-multi-prefix-sort-8thread.cu:279-325,446-452). */
+typedef struct {
+  char name[32];
+  uint64_t launches;
+  double total_ms;
+} hm_stage_time;
+
+/* Turns stage timing on (1) or off (0) for tree t; off by default. */
+int hm_profile(hm_tree *t, int enable);
+/* Waits for the recorded events, writes up to cap stage totals to out,
+ * sets *n, and clears the record. */
+int hm_profile_read(hm_tree *t, hm_stage_time *out, int cap, int *n);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,178 @@
+// Test infrastructure only: a small C-ABI driver around the reference CPU
+// B+tree (open-harmonia/src), compiled from the reference's own sources by
+// oracle/Makefile into oracle/_ref/libhmref.so.  Only tests, the smoke check
+// and bench.py's reference/cpu_baseline arm load it; the product library
+// never does.
+//
+// The reference has no library API: its experiments are `main` plus one
+// function per CLI option (open-harmonia/src/main.cpp:50-67,166-414).  This
+// file re-hosts exactly the calls those experiments make, so that the oracle
+// is the reference's own code path:
+//   build   : BPlusTree::insert per key (main.cpp:56-66, bpt.cpp:357-409),
+//             then BPlusTree::sort -> PPI tree (main.cpp:151-152,
+//             traversal.cpp:35-129) with prefixArray (traversal.cpp:180-195)
+//   search  : search_cpu_test's OpenMP loop over BPlusTree::search
+//             (main.cpp:772-812, bpt.cpp:673-680, bpt-ppi.cpp:118-156);
+//             after an update the Newupdate descent
+//             (bpt-ppi-update.cpp:12-89), which also follows "normal" nodes
+//   range   : the PPI range traversal of cpu-range.cpp:129-183 with the
+//             end key forced to Max_Key (range.cu:349-355), generalised from
+//             Range_Size=8 to a per-query length, and stepping to the next
+//             big leaf through BLeaf_node::next (bpt.cpp:55-56) as
+//             BPlusTree::range_search does (bpt.cpp:695-769), which stays
+//             correct after updates append leaves out of order
+//   upsert  : BPlusTree::insert_parallel_Newupdate_batch
+//             (bpt-ppi-update-batch.cpp:86-200): an existing key's value
+//             becomes key-1, a new key is inserted with its supplied value
+//   export  : in-order walk of the big-leaf chain (bpt.h:241-337)
+#include "bpt.h"
+
+#include <omp.h>
+
+#include <cstdint>
+#include <vector>
+
+namespace {
+
+struct RefTree {
+  BPlusTree *ppi = nullptr;
+  bool updated = false;
+};
+
+BLeaf_node *leaf_for(BPlusTree *t, Inner_node *last, long long key,
+                     int &relist_idx) {
+  // Mirrors search_leaf_PPItree_Newupdate (bpt-ppi-update.cpp:40-59).
+  if (last == nullptr) {
+    relist_idx = 0;
+    return static_cast<BLeaf_node *>(t->getRoot());
+  }
+  relist_idx = last->getChildIdx(nullptr, key);
+  int idx = t->getInnerNodeIdx(last);
+  if (t->isNormalInnerNode(idx))
+    return static_cast<BLeaf_node *>(last->child[0]);
+  return t->getBLeafNodeByIdx(idx - t->getInnerSize_wo_last_inner_node());
+}
+
+}  // namespace
+
+extern "C" {
+
+int hmref_abi_version() { return 1; }
+
+// Returns nullptr when the reference cannot represent the tree: it needs at
+// least one inner node (sort() asserts the root is inner, traversal.cpp:87),
+// i.e. more than 4 distinct keys.
+void *hmref_build(const long long *keys, const long long *vals, long n) {
+  BPlusTree *tree = new BPlusTree();
+  for (long i = 0; i < n; i++) tree->insert(keys[i], vals[i]);
+  if (tree->getHeight() < 2) return nullptr;
+  RefTree *h = new RefTree();
+  tree->sort(h->ppi);
+  return h;
+}
+
+int hmref_height(void *hp) { return static_cast<RefTree *>(hp)->ppi->getHeight(); }
+long hmref_inner_nodes(void *hp) { return static_cast<RefTree *>(hp)->ppi->getInnerSize(); }
+long hmref_big_leaves(void *hp) { return static_cast<RefTree *>(hp)->ppi->getBLeafSize(); }
+
+// Point search; out[i] is the value or -1.  threads<=0 uses OpenMP's default.
+void hmref_search(void *hp, const long long *q, long n, long long *out,
+                  int threads) {
+  RefTree *h = static_cast<RefTree *>(hp);
+  BPlusTree *t = h->ppi;
+  int nt = threads > 0 ? threads : omp_get_max_threads();
+  if (!h->updated) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (long i = 0; i < n; i++) out[i] = t->search(q[i]);
+  } else {
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (long i = 0; i < n; i++) out[i] = t->search_PPItree_Newupdate(q[i]);
+  }
+}
+
+// Range: for query i, the first len[i] records with key >= start[i] in
+// ascending key order (fewer when the key space ends).  offsets has n+1
+// entries (exclusive scan of the per-query counts).  Returns the total number
+// of records, or -1 if cap is too small.
+long hmref_range(void *hp, const long long *start, const int *len, long n,
+                 long long *offsets, long long *okeys, long long *ovals,
+                 long cap) {
+  BPlusTree *t = static_cast<RefTree *>(hp)->ppi;
+  long total = 0;
+  for (long i = 0; i < n; i++) {
+    offsets[i] = total;
+    long want = len[i] > 0 ? len[i] : 0;
+    if (want == 0 || start[i] == Max_Key) continue;
+    Inner_node *last = t->search_last_level_inner_node_PPItree_Newupdate(start[i]);
+    int relist_idx = 0;
+    BLeaf_node *node = leaf_for(t, last, start[i], relist_idx);
+    int idx = node->findKeyLowerBound(relist_idx, start[i]);
+    if (idx < 0) {  // nothing >= start in this record list
+      idx = 0;
+      relist_idx++;
+    }
+    long got = 0;
+    while (node != nullptr && got < want) {
+      if (relist_idx >= node->used_relist_slot_num) {
+        node = node->next;
+        relist_idx = 0;
+        idx = 0;
+        continue;
+      }
+      if (idx >= node->size[relist_idx]) {
+        relist_idx++;
+        idx = 0;
+        continue;
+      }
+      if (total >= cap) return -1;
+      okeys[total] = node->relist[relist_idx].r[idx].r_key;
+      ovals[total] = node->relist[relist_idx].r[idx].val;
+      total++;
+      got++;
+      idx++;
+    }
+  }
+  offsets[n] = total;
+  return total;
+}
+
+// One update batch through the reference's parallel update.  syn_batch and
+// rebuild_batch are the reference's two batch sizes; the reference reads past
+// the input unless n is a multiple of syn_batch, so other values are clamped
+// to n.  Returns 0.
+int hmref_upsert(void *hp, const long long *keys, const long long *vals,
+                 long n, long syn_batch, long rebuild_batch) {
+  RefTree *h = static_cast<RefTree *>(hp);
+  if (n <= 0) return 0;
+  if (syn_batch <= 0 || n % syn_batch != 0) syn_batch = n;
+  if (rebuild_batch <= 0 || rebuild_batch % syn_batch != 0) rebuild_batch = syn_batch;
+  std::vector<key_t> k(keys, keys + n);
+  std::vector<value_t> v(vals, vals + n);
+  h->ppi->insert_parallel_Newupdate_batch(k, v, (int)syn_batch, (int)rebuild_batch);
+  h->updated = true;
+  return 0;
+}
+
+// Sorted (key, value) contents.  Returns the record count, or -1 if cap is
+// too small (the count is still walked so the caller can resize).
+long hmref_export(void *hp, long long *keys, long long *vals, long cap) {
+  BPlusTree *t = static_cast<RefTree *>(hp)->ppi;
+  long total = 0;
+  bool overflow = false;
+  for (BLeaf_node *node = t->getBLeafNodeByIdx(0); node != nullptr; node = node->next) {
+    for (int r = 0; r < node->used_relist_slot_num; r++) {
+      for (int j = 0; j < node->size[r]; j++) {
+        if (total < cap) {
+          keys[total] = node->relist[r].r[j].r_key;
+          vals[total] = node->relist[r].r[j].val;
+        } else {
+          overflow = true;
+        }
+        total++;
+      }
+    }
+  }
+  return overflow ? -1 : total;
+}
+
+}  // extern "C"

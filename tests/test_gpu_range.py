@@ -1,0 +1,77 @@
+"""GPU parity tests of the range scan with prefix-sum compaction."""
+import numpy as np
+import pytest
+
+from harmonia_b200 import BPlusTree, HarmoniaError, datagen as dg
+from oracle import pyoracle as po
+from tests.helpers import digest, load_golden, load_small
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+GOLD = load_golden()
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.fixture(scope="module")
+def c1():
+    g = GOLD["c1_point"]
+    keys = dg.gen_keys(g["n"], g["key_seed"])
+    sk = np.sort(keys)
+    t = BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)))
+    yield keys, sk, t
+    t.close()
+
+
+def test_c1_range_digest_device_and_host(c1):
+    keys, sk, t = c1
+    g = GOLD["c1_range"]
+    st, ln = dg.gen_ranges(g["m"], g["lo"], g["hi"], g["seed"])
+    off, k, v = t.range_search(cuda(st), cuda(ln))
+    assert digest(off.cpu().numpy(), k.cpu().numpy(), v.cpu().numpy()) == g["digest"]
+    off, k, v = t.range_search(st, ln)
+    assert digest(off, k, v) == g["digest"]
+
+
+@pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (64, 64), (128, 16), (128, 64)])
+def test_small_golden(fanout, leaf_cap):
+    s = load_small()
+    keys = dg.gen_keys(int(s["n"]), int(s["key_seed"]))
+    with BPlusTree.bulk_load(keys, dg.values_for(keys), fanout=fanout, leaf_cap=leaf_cap) as t:
+        off, k, v = t.range_search(s["r_start"], s["r_len"])
+        assert (off == s["r_off"]).all() and (k == s["r_keys"]).all() and (v == s["r_vals"]).all()
+
+
+def test_edge_ranges(c1):
+    keys, sk, t = c1
+    st = np.array([sk[0], sk[-1], sk[-1] + 1, 2**63 - 1, -(2**63), sk[5] + 1, sk[100], sk[-2]], np.int64)
+    ln = np.array([3, 5, 4, 9, 2, 0, -3, 1000], np.int32)
+    exp = po.PortTree(sk, dg.values_for(sk)).range(st, ln)
+    got = t.range_search(cuda(st), cuda(ln))
+    for a, b in zip(got, exp):
+        assert (a.cpu().numpy() == b).all()
+    assert exp[0][-1] == 3 + 1 + 0 + 0 + 2 + 0 + 0 + 2
+
+
+def test_capacity_error(c1):
+    keys, sk, t = c1
+    st = cuda(np.array([sk[0]], np.int64))
+    ln = cuda(np.array([10], np.int32))
+    import ctypes
+    from harmonia_b200 import native
+    off = torch.empty(2, dtype=torch.int64, device="cuda")
+    ok = torch.empty(4, dtype=torch.int64, device="cuda")
+    tot = ctypes.c_size_t()
+    rc = native.lib().hm_range(t.handle, st.data_ptr(), ln.data_ptr(), 1, off.data_ptr(), ok.data_ptr(),
+                               ok.data_ptr(), 4, ctypes.byref(tot), None)
+    assert rc == -6 and tot.value == 10
+
+
+def test_empty_tree_and_empty_batch():
+    with BPlusTree.bulk_load(np.zeros(0, np.int64), np.zeros(0, np.int64)) as t:
+        off, k, v = t.range_search(np.array([0, 5], np.int64), np.array([3, 3], np.int32))
+        assert off.tolist() == [0, 0, 0] and len(k) == 0
+        off, k, v = t.range_search(np.zeros(0, np.int64), np.zeros(0, np.int32))
+        assert off.tolist() == [0]

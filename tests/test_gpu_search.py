@@ -1,0 +1,185 @@
+"""GPU parity tests of the bulk loader and the point search, through the C ABI.
+
+Bit-exact against the oracle: the C restatement (layout and results) and the
+reference CPU tree's golden digests."""
+import numpy as np
+import pytest
+
+from harmonia_b200 import BPlusTree, HarmoniaError, datagen as dg, native
+from oracle import pyoracle as po
+from tests.helpers import digest, load_golden, load_small
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+GOLD = load_golden()
+CONFIGS = [(64, 16), (64, 64), (128, 16), (128, 64)]
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.fixture(scope="module")
+def c1():
+    g = GOLD["c1_point"]
+    keys = dg.gen_keys(g["n"], g["key_seed"])
+    vals = dg.values_for(keys)
+    sk = np.sort(keys)
+    t = BPlusTree.bulk_load(cuda(keys), cuda(vals))
+    yield keys, sk, t
+    t.close()
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 15, 16, 17, 64, 1000, 4097, 1 << 16])
+@pytest.mark.parametrize("fanout,leaf_cap", CONFIGS)
+def test_bulk_load_layout_bit_exact(n, fanout, leaf_cap):
+    keys = dg.gen_keys(n, seed=n + 5)
+    vals = dg.values_for(keys)
+    sk = np.sort(keys)
+    exp = po.PortTree(sk, dg.values_for(sk), fanout=fanout, leaf_cap=leaf_cap).layout()
+    with BPlusTree.bulk_load(keys, vals, fanout=fanout, leaf_cap=leaf_cap) as t:
+        got = t.layout()
+    for k in ("height", "lvl_start", "n_inner", "n_leaf"):
+        assert got[k] == exp[k], k
+    for k in ("inner", "prefix", "leaf_keys", "leaf_vals", "leaf_cnt", "leaf_base"):
+        assert (got[k] == exp[k]).all(), k
+
+
+@pytest.mark.parametrize("inner_fill,leaf_fill", [(2, 1), (3, 5), (33, 12), (64, 16)])
+def test_bulk_load_partial_fill_layout(inner_fill, leaf_fill):
+    keys = dg.gen_keys(20000, seed=9)
+    sk = np.sort(keys)
+    exp = po.PortTree(sk, dg.values_for(sk), 64, 16, inner_fill, leaf_fill).layout()
+    with BPlusTree.bulk_load(keys, dg.values_for(keys), 64, 16, inner_fill, leaf_fill) as t:
+        got = t.layout()
+    for k in ("inner", "prefix", "leaf_keys", "leaf_vals", "leaf_cnt", "leaf_base"):
+        assert (got[k] == exp[k]).all(), k
+
+
+def test_c1_point_digest(c1):
+    keys, sk, t = c1
+    g = GOLD["c1_point"]
+    q = dg.gen_point_queries(keys, g["m"], g["hit"], g["q_seed"])
+    out = t.search(cuda(q)).cpu().numpy()
+    assert digest(out) == g["digest"]
+
+
+def test_c1_zipf_digest(c1):
+    keys, sk, t = c1
+    g = GOLD["c1_zipf"]
+    q = dg.gen_zipf_queries(sk, g["m"], g["theta"], g["q_seed"])
+    assert digest(t.search(cuda(q)).cpu().numpy()) == g["digest"]
+
+
+@pytest.mark.parametrize("w", [1, 2, 4, 8, 16, 32])
+@pytest.mark.parametrize("qpg", [1, 2, 4])
+def test_every_group_width_and_depth(c1, w, qpg):
+    keys, sk, t = c1
+    q = dg.gen_point_queries(keys, 300001, 0.7, seed=w * 10 + qpg)
+    exp = po.PortTree(sk, dg.values_for(sk)).search(q)
+    t.set_search_config(group_width=w, queries_per_group=qpg, sort_bits=0)
+    try:
+        assert (t.search(cuda(q)).cpu().numpy() == exp).all()
+    finally:
+        t.set_search_config(group_width=4, queries_per_group=2, sort_bits=-1)
+
+
+@pytest.mark.parametrize("bits", [1, 4, 8, 12])
+def test_presort_bits(c1, bits):
+    keys, sk, t = c1
+    q = dg.gen_point_queries(keys, 1 << 19, 0.9, seed=bits)
+    exp = po.PortTree(sk, dg.values_for(sk)).search(q)
+    t.set_search_config(sort_bits=bits)
+    try:
+        assert (t.search(cuda(q)).cpu().numpy() == exp).all()
+    finally:
+        t.set_search_config(sort_bits=-1)
+
+
+@pytest.mark.parametrize("fanout,leaf_cap", CONFIGS)
+def test_configs_against_small_golden(fanout, leaf_cap):
+    s = load_small()
+    keys = dg.gen_keys(int(s["n"]), int(s["key_seed"]))
+    with BPlusTree.bulk_load(keys, dg.values_for(keys), fanout=fanout, leaf_cap=leaf_cap) as t:
+        assert (t.search(cuda(s["q"])).cpu().numpy() == s["res"]).all()
+        assert (t.search(s["q"]) == s["res"]).all()  # host buffers
+
+
+def test_host_pageable_and_pinned_buffers(c1):
+    keys, sk, t = c1
+    q = dg.gen_point_queries(keys, (1 << 22) * 2 + 12345, 0.5, seed=77)  # > 2 pipeline chunks
+    exp = po.PortTree(sk, dg.values_for(sk)).search(q)
+    assert (t.search(q) == exp).all()
+    qp = torch.from_numpy(q).pin_memory()
+    op = torch.empty_like(qp).pin_memory()
+    t.search(qp, op)
+    assert (op.numpy() == exp).all()
+
+
+def test_edge_queries(c1):
+    keys, sk, t = c1
+    q = np.array([sk[0], sk[-1], sk[0] - 1, sk[-1] + 1, -(2**63), 2**63 - 1, -1, 0], dtype=np.int64)
+    exp = po.PortTree(sk, dg.values_for(sk)).search(q)
+    assert exp[-3] == -1 and exp[2] == -1
+    for n in (1, 3, len(q)):
+        assert (t.search(cuda(q[:n])).cpu().numpy() == exp[:n]).all()
+    assert len(t.search(cuda(q[:0]))) == 0
+
+
+def test_negative_and_extreme_keys():
+    keys = np.array([-(2**63), -5, -1, 0, 7, 2**63 - 2], dtype=np.int64)
+    vals = np.arange(6, dtype=np.int64) * 3
+    with BPlusTree.bulk_load(keys[::-1].copy(), vals[::-1].copy()) as t:
+        q = np.concatenate([keys, [-4, 1, 2**63 - 1, 8]])
+        got = t.search(cuda(q)).cpu().numpy()
+        assert got.tolist() == vals.tolist() + [-1, -1, -1, -1]
+
+
+def test_empty_and_single_key_trees():
+    with BPlusTree.bulk_load(np.zeros(0, np.int64), np.zeros(0, np.int64)) as t:
+        assert (t.search(cuda(np.array([0, 5, -5], np.int64))).cpu().numpy() == -1).all()
+        assert t.size == 0
+    with BPlusTree.bulk_load(np.array([42], np.int64), np.array([7], np.int64)) as t:
+        assert t.search(cuda(np.array([42, 41, 43], np.int64))).cpu().tolist() == [7, -1, -1]
+
+
+def test_bulk_load_errors():
+    with pytest.raises(HarmoniaError) as e:
+        BPlusTree.bulk_load(np.array([3, 1, 3], np.int64), np.zeros(3, np.int64))
+    assert e.value.code == -3
+    with pytest.raises(HarmoniaError) as e:
+        BPlusTree.bulk_load(np.array([1, 2**63 - 1], np.int64), np.zeros(2, np.int64))
+    assert e.value.code == -4
+    with pytest.raises(HarmoniaError) as e:
+        BPlusTree.bulk_load(np.array([1], np.int64), np.zeros(1, np.int64), fanout=96)
+    assert e.value.code == -1
+
+
+def test_search_batches_uneven(c1):
+    keys, sk, t = c1
+    oracle = po.PortTree(sk, dg.values_for(sk))
+    sizes = [1, 2, 255, 256, 257, 1000, 4096, 70001, 3, 0, 12345]
+    qs = [dg.gen_point_queries(keys, m, 0.5, seed=300 + i) for i, m in enumerate(sizes)]
+    dq = [cuda(q) for q in qs]
+    outs = [torch.full((len(q),), -77, dtype=torch.int64, device="cuda") for q in qs]
+    t.search_batches(list(zip(dq, outs)))
+    for q, o in zip(qs, outs):
+        assert (o.cpu().numpy() == oracle.search(q)).all()
+
+
+def test_autotune_keeps_results_exact(c1):
+    keys, sk, t = c1
+    q = dg.gen_point_queries(keys, 1 << 18, 0.9, seed=5)
+    best = t.autotune(cuda(q))
+    assert best["group_width"] in (2, 4, 8, 16, 32)
+    exp = po.PortTree(sk, dg.values_for(sk)).search(q)
+    assert (t.search(cuda(q)).cpu().numpy() == exp).all()
+    t.set_search_config(group_width=4, queries_per_group=2, sort_bits=-1)
+
+
+def test_launches_come_from_the_library(c1):
+    keys, sk, t = c1
+    before = native.lib().hm_launch_count()
+    t.search(cuda(keys[:1000]))
+    torch.cuda.synchronize()
+    assert native.lib().hm_launch_count() > before

@@ -1,0 +1,100 @@
+"""GPU parity tests of the epoch upsert (in-place merge and rebuild paths)."""
+import numpy as np
+import pytest
+
+from harmonia_b200 import BPlusTree, HarmoniaError, datagen as dg
+from oracle import pyoracle as po
+from tests.helpers import digest, load_golden, load_small
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+GOLD = load_golden()
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("leaf_fill", [12, 16])
+def test_c1_two_epochs_match_reference(leaf_fill):
+    g0, g1, g2 = GOLD["c1_point"], GOLD["c1_upsert"], GOLD["c1_upsert2"]
+    keys = dg.gen_keys(g0["n"], g0["key_seed"])
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), leaf_fill=leaf_fill) as t:
+        bk, bv = dg.gen_upserts(keys, g1["m"], g1["new_frac"], g1["seed"])
+        t.upsert(cuda(bk), cuda(bv))
+        ek, ev = t.export()
+        assert len(ek) == g1["n_after"] and digest(ek, ev) == g1["export_digest"]
+        assert digest(t.search(cuda(bk)).cpu().numpy()) == g1["search_digest"]
+        bk2, bv2 = dg.gen_upserts(ek, g2["m"], g2["new_frac"], g2["seed"])
+        t.upsert(bk2, bv2)  # host buffers
+        ek2, ev2 = t.export()
+        assert digest(ek2, ev2) == g2["export_digest"]
+        assert digest(t.search(cuda(bk2)).cpu().numpy()) == g2["search_digest"]
+
+
+def test_small_golden_reference_rule():
+    s = load_small()
+    keys = dg.gen_keys(int(s["n"]), int(s["key_seed"]))
+    with BPlusTree.bulk_load(keys, dg.values_for(keys), fanout=128, leaf_cap=64, leaf_fill=40) as t:
+        # the reference's rule ignores the supplied value of existing keys
+        vals = np.where(np.isin(s["u_keys"], keys), 999, s["u_vals"])
+        t.insert_parallel_Newupdate_batch(vals * 0 + s["u_keys"], vals)
+        ek, ev = t.export()
+        assert (ek == s["after_keys"]).all() and (ev == s["after_vals"]).all()
+
+
+def test_duplicates_in_batch_last_wins():
+    keys = np.arange(0, 2000, 2, dtype=np.int64)
+    with BPlusTree.bulk_load(keys, keys * 10) as t:
+        bk = np.array([4, 5, 4, 5, 7, 1999], np.int64)
+        bv = np.array([1, 2, 3, 4, 5, 6], np.int64)
+        t.upsert(bk, bv)
+        ek, ev = po.upsert_set(keys, keys * 10, bk, bv)
+        xk, xv = t.export()
+        assert (xk == ek).all() and (xv == ev).all()
+        assert t.search(cuda(np.array([4, 5, 7, 1999, 3], np.int64))).cpu().tolist() == [3, 4, 5, 6, -1]
+
+
+@pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (128, 64)])
+def test_overflow_triggers_rebuild(fanout, leaf_cap):
+    keys = dg.gen_keys(5000, seed=31)
+    vals = dg.values_for(keys)
+    with BPlusTree.bulk_load(keys, vals, fanout=fanout, leaf_cap=leaf_cap) as t:  # full leaves
+        h0 = t.info().n_leaf
+        bk, bv = dg.gen_upserts(keys, 6000, 0.9, seed=32)
+        t.upsert(bk, bv)
+        sk = np.sort(keys)
+        ek, ev = po.upsert_set(sk, dg.values_for(sk), bk, bv)
+        xk, xv = t.export()
+        assert (xk == ek).all() and (xv == ev).all()
+        assert t.info().n_leaf > h0
+        q = np.concatenate([bk, dg.gen_point_queries(keys, 5000, 0.5, seed=33)])
+        assert (t.search(cuda(q)).cpu().numpy() == po.PortTree(ek, ev).search(q)).all()
+        st, ln = dg.gen_ranges(300, 1, 100, seed=34)
+        got = t.range_search(st, ln)
+        exp = po.PortTree(ek, ev).range(st, ln)
+        assert all((a == b).all() for a, b in zip(got, exp))
+
+
+def test_upsert_into_empty_tree_and_errors():
+    with BPlusTree.bulk_load(np.zeros(0, np.int64), np.zeros(0, np.int64)) as t:
+        bk = np.array([5, -3, 100], np.int64)
+        t.upsert(bk, bk + 1)
+        k, v = t.export()
+        assert k.tolist() == [-3, 5, 100] and v.tolist() == [-2, 6, 101]
+        with pytest.raises(HarmoniaError) as e:
+            t.upsert(np.array([1, 2**63 - 1], np.int64), np.zeros(2, np.int64))
+        assert e.value.code == -4
+        assert t.export()[0].tolist() == [-3, 5, 100]
+
+
+def test_many_small_epochs_stay_exact():
+    keys = dg.gen_keys(1 << 14, seed=41)
+    sk, sv = np.sort(keys), dg.values_for(np.sort(keys))
+    with BPlusTree.bulk_load(keys, dg.values_for(keys), leaf_fill=12) as t:
+        for e in range(12):
+            bk, bv = dg.gen_upserts(sk, 700, 0.5, seed=50 + e)
+            t.upsert(cuda(bk), cuda(bv))
+            sk, sv = po.upsert_set(sk, sv, bk, bv)
+        xk, xv = t.export()
+        assert (xk == sk).all() and (xv == sv).all()

@@ -1,0 +1,147 @@
+"""CPU tests of the oracle: the C restatement is pinned to the reference's own
+CPU B+tree through the golden fixtures (and directly, where the reference
+library is built in this checkout)."""
+import numpy as np
+import pytest
+
+from harmonia_b200 import datagen as dg
+from oracle import pyoracle as po
+from tests.helpers import digest, load_golden, load_small
+
+GOLD = load_golden()
+
+
+def test_splitmix64_numpy_matches_c():
+    xs = np.array([0, 1, 2, 12345, 2**63 - 1, 2**64 - 1], dtype=np.uint64)
+    got = dg.splitmix64(xs)
+    assert [int(g) for g in got] == [po.splitmix64(int(x)) for x in xs]
+
+
+def test_generated_keys_distinct_and_sentinel_free():
+    k = dg.gen_keys(1 << 18, seed=3)
+    assert len(np.unique(k)) == len(k)
+    assert (k >= 0).all() and (k != dg.MAX_KEY).all()
+    assert (dg.values_for(k) >= 0).all()
+    assert (dg.gen_keys(1000, seed=3) == k[:1000]).all()  # prefix-stable, seeded
+
+
+def test_port_matches_small_golden():
+    s = load_small()
+    keys = dg.gen_keys(int(s["n"]), int(s["key_seed"]))
+    sk = np.sort(keys)
+    for fanout, leaf_cap in [(64, 16), (64, 64), (128, 16), (128, 64)]:
+        t = po.PortTree(sk, dg.values_for(sk), fanout=fanout, leaf_cap=leaf_cap)
+        assert (t.search(s["q"]) == s["res"]).all()
+        off, k, v = t.range(s["r_start"], s["r_len"])
+        assert (off == s["r_off"]).all() and (k == s["r_keys"]).all() and (v == s["r_vals"]).all()
+    ek, ev = po.upsert_set(sk, dg.values_for(sk), s["u_keys"], s["u_vals"])
+    assert (ek == s["after_keys"]).all() and (ev == s["after_vals"]).all()
+
+
+@pytest.fixture(scope="module")
+def c1():
+    g = GOLD["c1_point"]
+    keys = dg.gen_keys(g["n"], g["key_seed"])
+    sk = np.sort(keys)
+    return keys, sk, dg.values_for(sk)
+
+
+def test_port_matches_c1_point_digest(c1):
+    keys, sk, sv = c1
+    g = GOLD["c1_point"]
+    q = dg.gen_point_queries(keys, g["m"], g["hit"], g["q_seed"])
+    out = po.PortTree(sk, sv).search(q)
+    assert digest(out) == g["digest"]
+    assert int((out >= 0).sum()) == g["hits"]
+
+
+def test_port_matches_c1_zipf_and_range_digests(c1):
+    keys, sk, sv = c1
+    t = po.PortTree(sk, sv, fanout=128, leaf_cap=64)
+    g = GOLD["c1_zipf"]
+    q = dg.gen_zipf_queries(sk, g["m"], g["theta"], g["q_seed"])
+    assert digest(t.search(q)) == g["digest"]
+    g = GOLD["c1_range"]
+    st, ln = dg.gen_ranges(g["m"], g["lo"], g["hi"], g["seed"])
+    off, k, v = t.range(st, ln)
+    assert digest(off, k, v) == g["digest"]
+
+
+def test_port_matches_c1_upsert_digests(c1):
+    keys, sk, sv = c1
+    g1, g2 = GOLD["c1_upsert"], GOLD["c1_upsert2"]
+    bk, bv = dg.gen_upserts(keys, g1["m"], g1["new_frac"], g1["seed"])
+    ek, ev = po.upsert_set(sk, sv, bk, bv)
+    assert len(ek) == g1["n_after"] and digest(ek, ev) == g1["export_digest"]
+    assert digest(po.PortTree(ek, ev).search(bk)) == g1["search_digest"]
+    bk2, bv2 = dg.gen_upserts(ek, g2["m"], g2["new_frac"], g2["seed"])
+    ek2, ev2 = po.upsert_set(ek, ev, bk2, bv2)
+    assert digest(ek2, ev2) == g2["export_digest"]
+    assert digest(po.PortTree(ek2, ev2).search(bk2)) == g2["search_digest"]
+
+
+def test_reference_rule_upsert_equals_supplied_key_minus_1(c1):
+    keys, sk, sv = c1
+    bk, bv = dg.gen_upserts(keys, 4096, 0.5, 21)
+    a = po.upsert_set(sk, sv, bk, bv)
+    b = po.upsert_set(sk, sv, bk, np.where(np.isin(bk, sk), 12345, bv), ref_rule=True)
+    assert (a[0] == b[0]).all() and (a[1] == b[1]).all()
+
+
+def test_upsert_last_occurrence_wins():
+    sk = np.array([10, 20, 30], np.int64)
+    sv = np.array([1, 2, 3], np.int64)
+    k, v = po.upsert_set(sk, sv, np.array([20, 5, 20, 5], np.int64), np.array([7, 8, 9, 10], np.int64))
+    assert k.tolist() == [5, 10, 20, 30] and v.tolist() == [10, 1, 9, 3]
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 15, 16, 17, 63, 64, 65, 1000, 4097])
+@pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (128, 64)])
+def test_port_layout_invariants(n, fanout, leaf_cap):
+    keys = np.sort(dg.gen_keys(n, seed=n + 1))
+    vals = dg.values_for(keys)
+    t = po.PortTree(keys, vals, fanout=fanout, leaf_cap=leaf_cap)
+    L = t.layout()
+    h, ls, ni, nl = po.shape(n, fanout, leaf_cap)
+    assert (L["height"], L["lvl_start"], L["n_inner"], L["n_leaf"]) == (h, ls, ni, nl)
+    row = fanout // 8 + fanout
+    inner = L["inner"].reshape(ni, row)
+    # prefix is the running sum of child counts (CFB: prefix[i+1] = prefix[i] + children_i)
+    nchild = [int((inner[i, fanout // 8:] != po.MAX_KEY).sum()) + 1 for i in range(ni)]
+    assert L["prefix"][0] == 1 or ni == 1 and L["prefix"][0] == ni
+    for i in range(ni - 1):
+        assert L["prefix"][i + 1] == L["prefix"][i] + nchild[i]
+    assert L["prefix"][ni - 1] + nchild[ni - 1] == ni + nl
+    # index words mirror every 8th key
+    for i in range(ni):
+        for j in range(fanout // 8):
+            s = 8 * (j + 1)
+            assert inner[i, j] == (inner[i, fanout // 8 + s] if s < fanout else po.MAX_KEY)
+    assert int(L["leaf_cnt"].sum()) == n
+    assert (np.concatenate([[0], np.cumsum(L["leaf_cnt"])[:-1]]) == L["leaf_base"]).all()
+    ek, ev = t.export()
+    assert (ek == keys).all() and (ev == vals).all()
+    if n:
+        q = np.concatenate([keys, keys + 1, [np.int64(-(2**63)), po.MAX_KEY]])
+        exp = np.concatenate([vals, np.where(np.isin(keys + 1, keys), -1, -1), [-1, -1]])
+        exp[n:2 * n] = np.where(np.isin(keys + 1, keys), np.interp(keys + 1, keys, vals).astype(np.int64), -1)
+        assert (t.search(q)[:n] == vals).all()
+        assert (t.search(q)[-2:] == -1).all()
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference library not built in this checkout")
+@pytest.mark.parametrize("n", [5, 100, 5000, 1 << 16])
+@pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (64, 64), (128, 16), (128, 64)])
+def test_port_matches_reference_directly(n, fanout, leaf_cap):
+    keys = dg.gen_keys(n, seed=100 + n)
+    vals = dg.values_for(keys)
+    ref = po.RefTree(keys, vals)
+    sk = np.sort(keys)
+    t = po.PortTree(sk, dg.values_for(sk), fanout=fanout, leaf_cap=leaf_cap)
+    q = dg.gen_point_queries(keys, 20000, 0.5, seed=n)
+    q[:3] = [sk[0], sk[-1], -7]
+    assert (ref.search(q) == t.search(q)).all()
+    st, ln = dg.gen_ranges(500, 1, 300, seed=n)
+    st[:2] = [sk[0], sk[-1]]
+    a, b = ref.range(st, ln), t.range(st, ln)
+    assert all((x == y).all() for x, y in zip(a, b))
