@@ -49,25 +49,28 @@ __global__ void check_sorted_kernel(const uint64_t *__restrict__ u, int64_t n, u
   if (f) atomicOr(flags, f);
 }
 
-// One thread per (leaf, word) of the leaf key rows and value rows.
+// One thread per (leaf, word) of the leaf rows: index words, keys, values.
 __global__ void leaf_kernel(const uint64_t *__restrict__ u, const int64_t *__restrict__ vals,
                             int64_t n, int64_t n_leaf, int lc, int li,
-                            int64_t *__restrict__ leaf_keys, int64_t *__restrict__ leaf_vals,
-                            int32_t *__restrict__ leaf_cnt, int64_t *__restrict__ leaf_base,
-                            int64_t *__restrict__ submin) {
-  const int row = li + lc;
+                            int64_t *__restrict__ leaf_rows, int32_t *__restrict__ leaf_cnt,
+                            int64_t *__restrict__ leaf_base, int64_t *__restrict__ submin) {
+  const int row = li + 2 * lc;
   const int64_t total = n_leaf * (int64_t)row;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     int64_t j = t / row;
     int w = (int)(t - j * row);
     int64_t s = part_start(j, n, n_leaf), e = part_start(j + 1, n, n_leaf);
+    if (w >= li + lc) {  // value word
+      int slot = w - li - lc;
+      leaf_rows[t] = (s + slot < e) ? vals[s + slot] : (int64_t)HM_NOT_FOUND;
+      continue;
+    }
     int slot = w < li ? 8 * (w + 1) : w - li;  // index word w mirrors key slot 8(w+1)
     int64_t k = kMaxKey;
     if (slot < lc && s + slot < e) k = (int64_t)(u[s + slot] ^ kSign);
-    leaf_keys[t] = k;
+    leaf_rows[t] = k;
     if (w >= li) {
-      leaf_vals[j * lc + slot] = (s + slot < e) ? vals[s + slot] : (int64_t)HM_NOT_FOUND;
       if (slot == 0) {
         leaf_cnt[j] = (int32_t)(e - s);
         leaf_base[j] = s;
@@ -154,8 +157,7 @@ int build_from_sorted(hm_tree *t, const uint64_t *ukeys, const int64_t *vals, in
   const int lc = t->cfg.leaf_cap, f = t->cfg.fanout;
   int64_t leaf_words = t->n_leaf * (int64_t)t->leaf_row;
   leaf_kernel<<<min(blocks_for(leaf_words), 148u * 32), kThreads, 0, s>>>(
-      ukeys, vals, n, t->n_leaf, lc, t->leaf_index, t->leaf_keys, t->leaf_vals, t->leaf_cnt,
-      t->leaf_base, tmp_a);
+      ukeys, vals, n, t->n_leaf, lc, t->leaf_index, t->leaf_rows, t->leaf_cnt, t->leaf_base, tmp_a);
   note_launch();
   int64_t *below = tmp_a, *here = tmp_b;
   int64_t m = t->n_leaf;

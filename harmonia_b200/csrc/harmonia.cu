@@ -297,14 +297,13 @@ int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_c
   t->n_keys = n;
   t->inner_row = cfg.fanout / 8 + cfg.fanout;
   t->leaf_index = cfg.leaf_cap >= 32 ? cfg.leaf_cap / 8 : 0;
-  t->leaf_row = t->leaf_index + cfg.leaf_cap;
+  t->leaf_row = t->leaf_index + 2 * cfg.leaf_cap;
 
   // Arena: every array 256-B aligned; prefix padded to a multiple of 4.
   size_t off_inner = 0;
   size_t off_prefix = off_inner + align_up(t->n_inner * t->inner_row * 8, 256);
-  size_t off_lkeys = off_prefix + align_up(align_up(t->n_inner, 4) * 4, 256);
-  size_t off_lvals = off_lkeys + align_up(t->n_leaf * t->leaf_row * 8, 256);
-  size_t off_lcnt = off_lvals + align_up(t->n_leaf * cfg.leaf_cap * 8, 256);
+  size_t off_lrows = off_prefix + align_up(align_up(t->n_inner, 4) * 4, 256);
+  size_t off_lcnt = off_lrows + align_up(t->n_leaf * t->leaf_row * 8, 256);
   size_t off_lbase = off_lcnt + align_up(t->n_leaf * 4, 256);
   size_t total = off_lbase + align_up(t->n_leaf * 8, 256);
 
@@ -325,8 +324,7 @@ int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_c
   char *base = static_cast<char *>(t->arena);
   t->inner = reinterpret_cast<int64_t *>(base + off_inner);
   t->prefix = reinterpret_cast<int32_t *>(base + off_prefix);
-  t->leaf_keys = reinterpret_cast<int64_t *>(base + off_lkeys);
-  t->leaf_vals = reinterpret_cast<int64_t *>(base + off_lvals);
+  t->leaf_rows = reinterpret_cast<int64_t *>(base + off_lrows);
   t->leaf_cnt = reinterpret_cast<int32_t *>(base + off_lcnt);
   t->leaf_base = reinterpret_cast<int64_t *>(base + off_lbase);
 
@@ -407,8 +405,7 @@ int hm_tree_get_info(const hm_tree *t, hm_tree_info *info) {
   for (int i = 0; i <= t->height && i <= kMaxLevels; i++) info->lvl_start[i] = t->lvl_start[i];
   info->inner = t->inner;
   info->prefix = t->prefix;
-  info->leaf_keys = t->leaf_keys;
-  info->leaf_vals = t->leaf_vals;
+  info->leaf_rows = t->leaf_rows;
   info->leaf_cnt = t->leaf_cnt;
   info->leaf_base = t->leaf_base;
   info->device_bytes = t->arena_bytes;

@@ -13,9 +13,13 @@
 //             prefix[i] + c.  Children of the last inner level are numbered
 //             from n_inner, leaf j = id - n_inner (CFB prefix[] and
 //             idx - internal_node_num, open-harmonia/regular_bpt/cfb.cpp:21-32).
-//   leaf_keys n_leaf rows of (LI + LC) int64, LI = LC/8 index words when
-//             LC >= 32 (else 0), then LC key slots.
-//   leaf_vals n_leaf * LC int64, -1 in unused slots.
+//   leaf_rows n_leaf rows of (LI + 2*LC) int64: LI = LC/8 index words when
+//             LC >= 32 (else 0), LC key slots (Max_Key when unused), then the
+//             LC values of those keys (-1 when unused).  Keys and values of a
+//             leaf share one 256-B aligned record for LC = 16, so a hit reads
+//             its value from the DRAM page its keys came from (the reference's
+//             Record_list also keeps key and value together,
+//             open-harmonia/src/bpt.h:206-239).
 //   leaf_cnt  n_leaf int32 keys per leaf; leaf_base n_leaf int64 exclusive scan.
 #pragma once
 
@@ -41,8 +45,7 @@ enum : unsigned {
 struct DevTree {
   const int64_t *inner;
   const int32_t *prefix;
-  const int64_t *leaf_keys;
-  const int64_t *leaf_vals;
+  const int64_t *leaf_rows;
   const int32_t *leaf_cnt;
   const int64_t *leaf_base;
   int64_t n_keys;
@@ -82,8 +85,7 @@ struct hm_tree {
   size_t arena_bytes = 0;
   int64_t *inner = nullptr;
   int32_t *prefix = nullptr;
-  int64_t *leaf_keys = nullptr;
-  int64_t *leaf_vals = nullptr;
+  int64_t *leaf_rows = nullptr;
   int32_t *leaf_cnt = nullptr;
   int64_t *leaf_base = nullptr;
   // per-tree scratch (grown on demand), error word, pinned staging
@@ -107,8 +109,7 @@ struct hm_tree {
     hm::DevTree d;
     d.inner = inner;
     d.prefix = prefix;
-    d.leaf_keys = leaf_keys;
-    d.leaf_vals = leaf_vals;
+    d.leaf_rows = leaf_rows;
     d.leaf_cnt = leaf_cnt;
     d.leaf_base = leaf_base;
     d.n_keys = n_keys;

@@ -82,8 +82,9 @@ __global__ void export_kernel(DevTree t, int lc, int li, int64_t *__restrict__ k
     int s = (int)(x - j * lc);
     if (s < t.leaf_cnt[j]) {
       int64_t o = t.leaf_base[j] + s;
-      keys[o] = t.leaf_keys[j * (li + lc) + li + s];
-      vals[o] = t.leaf_vals[j * lc + s];
+      const int64_t *r = t.leaf_rows + j * (li + 2 * lc) + li;
+      keys[o] = r[s];
+      vals[o] = r[lc + s];
     }
   }
 }
@@ -125,7 +126,7 @@ __global__ void range_locate_kernel(DevTree t, int f, int lc, int li, const int6
       continue;
     }
     int32_t leaf = descend_scalar(t, f, s);
-    const int64_t *kr = t.leaf_keys + (int64_t)leaf * (li + lc) + li;
+    const int64_t *kr = t.leaf_rows + (int64_t)leaf * (li + 2 * lc) + li;
     int cnt = __ldg(t.leaf_cnt + leaf);
     int lb = 0;  // first slot with key >= start
     while (lb < cnt && __ldg(kr + lb) < s) lb++;
@@ -151,8 +152,8 @@ __global__ void range_copy_kernel(DevTree t, int lc, int li, const int32_t *__re
     while (rem > 0 && leaf < t.n_leaf) {
       int avail = __ldg(t.leaf_cnt + leaf) - slot;
       int take = (int)(avail < rem ? avail : rem);
-      const int64_t *kr = t.leaf_keys + (int64_t)leaf * (li + lc) + li + slot;
-      const int64_t *vr = t.leaf_vals + (int64_t)leaf * lc + slot;
+      const int64_t *kr = t.leaf_rows + (int64_t)leaf * (li + 2 * lc) + li + slot;
+      const int64_t *vr = kr + lc;
       for (int x = lane; x < take; x += 32) {
         okeys[o + x] = __ldg(kr + x);
         ovals[o + x] = __ldg(vr + x);

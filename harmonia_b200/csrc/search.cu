@@ -214,7 +214,7 @@ __device__ __forceinline__ void search_tile(const DevTree &t, const int64_t *sro
   constexpr int G = kThreads / W;   // groups per CTA
   constexpr int ROW = F / 8 + F;    // inner row words
   constexpr int LI = LC >= 32 ? LC / 8 : 0;
-  constexpr int LROW = LI + LC;
+  constexpr int LROW = LI + 2 * LC;
   const int gid = threadIdx.x / W, sub = threadIdx.x % W;
   const int lane = threadIdx.x & 31;
   const uint64_t pol_inner = t.cache_hints == 1 ? policy_evict_last() : policy_evict_normal();
@@ -261,7 +261,7 @@ __device__ __forceinline__ void search_tile(const DevTree &t, const int64_t *sro
 #pragma unroll
   for (int j = 0; j < Q; j++) {
     leaf[j] = node[j] - t.n_inner;
-    const int64_t *row = t.leaf_keys + (int64_t)leaf[j] * LROW;
+    const int64_t *row = t.leaf_rows + (int64_t)leaf[j] * LROW;
     if constexpr (LI == 0) {
       slot[j] = match_slot<W, LC>(row, key[j], sub, pol_leaf);
     } else {
@@ -278,7 +278,7 @@ __device__ __forceinline__ void search_tile(const DevTree &t, const int64_t *sro
     unsigned hit = __ballot_sync(0xffffffffu, slot[j] >= 0) & gmask;
     int writer = hit ? (__ffs(hit) - 1) : (lane & ~(W - 1));
     if (lane == writer && idx[j] < n) {
-      int64_t v = slot[j] >= 0 ? ldg1(t.leaf_vals + (int64_t)leaf[j] * LC + slot[j], pol_leaf)
+      int64_t v = slot[j] >= 0 ? ldg1(t.leaf_rows + (int64_t)leaf[j] * LROW + LI + LC + slot[j], pol_leaf)
                                : (int64_t)HM_NOT_FOUND;
       int64_t o = posp ? (int64_t)__ldg(posp + idx[j]) : idx[j];
       outp[o] = v;

@@ -131,14 +131,22 @@ __global__ void __launch_bounds__(kThreads) downsweep_kernel(
 
 }  // namespace
 
+// In-place exclusive scan of counts[0..m) (digit-major histograms).  Large
+// arrays go through the multi-CTA scan; the caller's buffer has room for
+// m + 1 entries plus scan_scratch_bytes(m) bytes after them.
 void scan_counts(int64_t *counts, int64_t m, cudaStream_t s) {
-  scan_counts_kernel<<<1, 1024, 0, s>>>(counts, m);
-  note_launch();
+  if (m <= 4096) {
+    scan_counts_kernel<<<1, 1024, 0, s>>>(counts, m);
+    note_launch();
+    return;
+  }
+  exclusive_scan_i64(counts, counts, m, counts + m + 1, s);
 }
 
 size_t radix_scratch_bytes(int64_t n) {
   (void)n;
-  return sizeof(int64_t) * (size_t)kBins * kMaxCtas;
+  const int64_t m = (int64_t)kBins * kMaxCtas;
+  return sizeof(int64_t) * (size_t)(m + 1) + scan_scratch_bytes(m) + 256;
 }
 
 template <typename V>
@@ -153,9 +161,10 @@ bool radix_sort_pairs(uint64_t *ukeys, V *vals, uint64_t *ukeys_alt, V *vals_alt
   bool flipped = false;
   for (int bit = begin_bit; bit < end_bit; bit += 8) {
     upsweep_kernel<<<nctas, kThreads, 0, s>>>(ka, n, seg, bit, counts, nctas);
-    scan_counts_kernel<<<1, 1024, 0, s>>>(counts, (int64_t)kBins * nctas);
+    note_launch(1);
+    scan_counts(counts, (int64_t)kBins * nctas, s);
     downsweep_kernel<V><<<nctas, kThreads, 0, s>>>(ka, va, kb, vb, n, seg, bit, counts, nctas);
-    note_launch(3);
+    note_launch(1);
     uint64_t *tk = ka;
     ka = kb;
     kb = tk;

@@ -94,20 +94,21 @@ __device__ __forceinline__ int32_t descend_to_leaf(const DevTree &t, int f, int6
 // Hits are updated in place; misses get miss[i] = 1 and their leaf.
 __global__ void apply_kernel(DevTree t, int f, int lc, int li, int flags,
                              const int64_t *__restrict__ bk, const int64_t *__restrict__ bv, int64_t m,
-                             int64_t *leaf_vals, int32_t *__restrict__ miss,
+                             int64_t *leaf_rows, int32_t *__restrict__ miss,
                              int32_t *__restrict__ leaf_of) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
        i += (int64_t)gridDim.x * blockDim.x) {
     int64_t k = bk[i];
     int32_t leaf = descend_to_leaf(t, f, k);
-    const int64_t *kr = t.leaf_keys + (int64_t)leaf * (li + lc) + li;
+    const int64_t *kr = t.leaf_rows + (int64_t)leaf * (li + 2 * lc) + li;
     int cnt = t.leaf_cnt[leaf];
     int slot = -1;
     for (int s = 0; s < cnt; s++)
       if (kr[s] == k) slot = s;
     leaf_of[i] = leaf;
     if (slot >= 0) {
-      leaf_vals[(int64_t)leaf * lc + slot] = (flags & HM_UPSERT_REF_KEY_MINUS_1) ? k - 1 : bv[i];
+      leaf_rows[(int64_t)leaf * (li + 2 * lc) + li + lc + slot] =
+          (flags & HM_UPSERT_REF_KEY_MINUS_1) ? k - 1 : bv[i];
       miss[i] = 0;
     } else {
       miss[i] = 1;
@@ -154,7 +155,7 @@ __global__ void miss_runs_kernel(const int32_t *__restrict__ ml, int64_t nm,
 }
 
 // One warp per run: merge the run's new keys into the leaf row.
-__global__ void merge_leaf_kernel(int64_t *leaf_keys, int64_t *leaf_vals, int32_t *leaf_cnt, int lc,
+__global__ void merge_leaf_kernel(int64_t *leaf_rows, int32_t *leaf_cnt, int lc,
                                   int li, const int64_t *__restrict__ mk, const int64_t *__restrict__ mv,
                                   const int32_t *__restrict__ is_start,
                                   const int64_t *__restrict__ run_start,
@@ -169,8 +170,8 @@ __global__ void merge_leaf_kernel(int64_t *leaf_keys, int64_t *leaf_vals, int32_
     const int32_t leaf = run_leaf[i];
     const int64_t r0 = run_start[i];
     const int rl = run_len[i];
-    int64_t *kr = leaf_keys + (int64_t)leaf * (li + lc) + li;
-    int64_t *vr = leaf_vals + (int64_t)leaf * lc;
+    int64_t *kr = leaf_rows + (int64_t)leaf * (li + 2 * lc) + li;
+    int64_t *vr = kr + lc;
     const int cnt = leaf_cnt[leaf];
     // existing key a goes to a + #(new < key); new key b to b + #(existing < key)
     for (int a = lane; a < cnt; a += 32) {
@@ -195,7 +196,7 @@ __global__ void merge_leaf_kernel(int64_t *leaf_keys, int64_t *leaf_vals, int32_
     }
     __syncwarp();
     if (li > 0) {
-      int64_t *ir = leaf_keys + (int64_t)leaf * (li + lc);
+      int64_t *ir = leaf_rows + (int64_t)leaf * (li + 2 * lc);
       for (int x = lane; x < li; x += 32) ir[x] = (8 * (x + 1) < lc) ? kr[8 * (x + 1)] : kMaxKey;
     }
     if (lane == 0) leaf_cnt[leaf] = nc;
@@ -283,7 +284,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   if (hf & 2u) return HM_EMAXKEY;
   const int64_t m = hm_[0];
 
-  apply_kernel<<<grid_for(m), kThreads, 0, s>>>(t->view(), f, lc, li, flags, bk, bv, m, t->leaf_vals,
+  apply_kernel<<<grid_for(m), kThreads, 0, s>>>(t->view(), f, lc, li, flags, bk, bv, m, t->leaf_rows,
                                                 miss, leaf_of);
   exclusive_scan_i32(miss, at, m, scan_scratch, s);
   compact_miss_kernel<<<grid_for(m), kThreads, 0, s>>>(bk, bv, leaf_of, miss, at, m, mk, mv, ml);
@@ -309,7 +310,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     // Every touched leaf has room: merge in place.
     int64_t blocks = (nm + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    merge_leaf_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(t->leaf_keys, t->leaf_vals, t->leaf_cnt, lc,
+    merge_leaf_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(t->leaf_rows, t->leaf_cnt, lc,
                                                             li, mk, mv, is_start, run_start, run_len,
                                                             run_leaf, nm);
     exclusive_scan_i32(t->leaf_cnt, at, t->n_leaf, scan_scratch, s);
@@ -330,9 +331,8 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     rc = shape(n1, t->cfg, &nt.height, nt.lvl_start, &nt.n_inner, &nt.n_leaf);
     if (rc) return rc;
     size_t off_prefix = al(nt.n_inner * nt.inner_row * 8);
-    size_t off_lkeys = off_prefix + al(align_up(nt.n_inner, 4) * 4);
-    size_t off_lvals = off_lkeys + al(nt.n_leaf * nt.leaf_row * 8);
-    size_t off_lcnt = off_lvals + al(nt.n_leaf * lc * 8);
+    size_t off_lrows = off_prefix + al(align_up(nt.n_inner, 4) * 4);
+    size_t off_lcnt = off_lrows + al(nt.n_leaf * nt.leaf_row * 8);
     size_t off_lbase = off_lcnt + al(nt.n_leaf * 4);
     size_t total = off_lbase + al(nt.n_leaf * 8);
     int64_t tn = std::max<int64_t>(std::max<int64_t>(n1, nt.n_leaf), 1);
@@ -359,8 +359,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     nt.arena_bytes = total;
     nt.inner = reinterpret_cast<int64_t *>(base);
     nt.prefix = reinterpret_cast<int32_t *>(base + off_prefix);
-    nt.leaf_keys = reinterpret_cast<int64_t *>(base + off_lkeys);
-    nt.leaf_vals = reinterpret_cast<int64_t *>(base + off_lvals);
+    nt.leaf_rows = reinterpret_cast<int64_t *>(base + off_lrows);
     nt.leaf_cnt = reinterpret_cast<int32_t *>(base + off_lcnt);
     nt.leaf_base = reinterpret_cast<int64_t *>(base + off_lbase);
     nt.n_keys = n1;
@@ -377,8 +376,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     t->arena_bytes = nt.arena_bytes;
     t->inner = nt.inner;
     t->prefix = nt.prefix;
-    t->leaf_keys = nt.leaf_keys;
-    t->leaf_vals = nt.leaf_vals;
+    t->leaf_rows = nt.leaf_rows;
     t->leaf_cnt = nt.leaf_cnt;
     t->leaf_base = nt.leaf_base;
     t->height = nt.height;

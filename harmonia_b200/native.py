@@ -54,7 +54,7 @@ class TreeInfo(ctypes.Structure):
                 ("n_keys", ctypes.c_int64), ("n_inner", ctypes.c_int64), ("n_leaf", ctypes.c_int64),
                 ("lvl_start", ctypes.c_int64 * 33),
                 ("inner", ctypes.c_void_p), ("prefix", ctypes.c_void_p),
-                ("leaf_keys", ctypes.c_void_p), ("leaf_vals", ctypes.c_void_p),
+                ("leaf_rows", ctypes.c_void_p),
                 ("leaf_cnt", ctypes.c_void_p), ("leaf_base", ctypes.c_void_p),
                 ("device_bytes", ctypes.c_size_t)]
 

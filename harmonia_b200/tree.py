@@ -244,8 +244,7 @@ class BPlusTree:
             "n_leaf": i.n_leaf,
             "inner": grab(i.inner, i.n_inner * i.inner_row_words, 8, np.int64),
             "prefix": grab(i.prefix, i.n_inner, 4, np.int32),
-            "leaf_keys": grab(i.leaf_keys, i.n_leaf * i.leaf_row_words, 8, np.int64),
-            "leaf_vals": grab(i.leaf_vals, i.n_leaf * i.leaf_cap, 8, np.int64),
+            "leaf_rows": grab(i.leaf_rows, i.n_leaf * i.leaf_row_words, 8, np.int64),
             "leaf_cnt": grab(i.leaf_cnt, i.n_leaf, 4, np.int32),
             "leaf_base": grab(i.leaf_base, i.n_leaf, 8, np.int64),
         }

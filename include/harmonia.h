@@ -77,7 +77,7 @@ typedef struct {
 typedef struct {
   int fanout, leaf_cap, height; /* height = number of inner levels */
   int inner_row_words;          /* int64 words per inner row: fanout/8 index + fanout keys */
-  int leaf_row_words;           /* int64 words per leaf key row */
+  int leaf_row_words;           /* int64 words per leaf row: index, leaf_cap keys, leaf_cap values */
   int leaf_index_words;         /* index words at the start of a leaf row (leaf_cap >= 32) */
   int smem_levels;              /* top levels staged in shared memory by the search kernel */
   int64_t n_keys, n_inner, n_leaf;
@@ -85,8 +85,7 @@ typedef struct {
   /* device pointers into the tree's HBM arena */
   const int64_t *inner;     /* n_inner rows */
   const int32_t *prefix;    /* n_inner first-child ids (leaves count from n_inner) */
-  const int64_t *leaf_keys; /* n_leaf rows */
-  const int64_t *leaf_vals; /* n_leaf * leaf_cap */
+  const int64_t *leaf_rows; /* n_leaf rows */
   const int32_t *leaf_cnt;  /* n_leaf */
   const int64_t *leaf_base; /* n_leaf, exclusive scan of leaf_cnt */
   size_t device_bytes;      /* bytes of the tree arena */

@@ -60,8 +60,7 @@ int hmo_shape(int64_t n, const hmo_params *p, int *height, int64_t *lvl_start,
 void hmo_free(hmo_tree *t) {
   free(t->inner);
   free(t->prefix);
-  free(t->leaf_keys);
-  free(t->leaf_vals);
+  free(t->leaf_rows);
   free(t->leaf_cnt);
   free(t->leaf_base);
   memset(t, 0, sizeof(*t));
@@ -81,18 +80,17 @@ int hmo_build(const int64_t *keys, const int64_t *vals, int64_t n,
   t->n_keys = n;
   t->inner_row = F / 8 + F;
   t->leaf_index = LC >= 32 ? LC / 8 : 0;
-  t->leaf_row = t->leaf_index + LC;
+  t->leaf_row = t->leaf_index + 2 * LC;
   t->inner = malloc(sizeof(int64_t) * t->n_inner * t->inner_row);
   t->prefix = malloc(sizeof(int32_t) * t->n_inner);
-  t->leaf_keys = malloc(sizeof(int64_t) * t->n_leaf * t->leaf_row);
-  t->leaf_vals = malloc(sizeof(int64_t) * t->n_leaf * LC);
+  t->leaf_rows = malloc(sizeof(int64_t) * t->n_leaf * t->leaf_row);
   t->leaf_cnt = malloc(sizeof(int32_t) * t->n_leaf);
   t->leaf_base = malloc(sizeof(int64_t) * t->n_leaf);
   /* first_leaf[] of the level being built: the leftmost leaf under each node,
    * whose first key is the node's subtree minimum. */
   int64_t *first_leaf = malloc(sizeof(int64_t) * t->n_leaf);
   int64_t *next_first = malloc(sizeof(int64_t) * t->n_leaf);
-  if (!t->inner || !t->prefix || !t->leaf_keys || !t->leaf_vals || !t->leaf_cnt ||
+  if (!t->inner || !t->prefix || !t->leaf_rows || !t->leaf_cnt ||
       !t->leaf_base || !first_leaf || !next_first) {
     free(first_leaf);
     free(next_first);
@@ -100,12 +98,15 @@ int hmo_build(const int64_t *keys, const int64_t *vals, int64_t n,
     return -4;
   }
 
-  /* Leaves: keys in order, evenly spread, Max_Key / -1 in empty slots. */
+  /* Leaves: keys in order, evenly spread, Max_Key / -1 in empty slots; each
+   * leaf row holds its keys and then their values, so a hit reads the value
+   * from the record it just compared (the reference's Record_list keeps key
+   * and value side by side too, open-harmonia/src/bpt.h:206-239). */
   for (int64_t j = 0; j < t->n_leaf; j++) {
     int64_t s = part_start(j, n, t->n_leaf), e = part_start(j + 1, n, t->n_leaf);
-    int64_t *row = t->leaf_keys + j * t->leaf_row;
+    int64_t *row = t->leaf_rows + j * t->leaf_row;
     int64_t *kr = row + t->leaf_index;
-    int64_t *vr = t->leaf_vals + j * LC;
+    int64_t *vr = kr + LC;
     for (int i = 0; i < LC; i++) {
       kr[i] = (s + i < e) ? keys[s + i] : HMO_MAX_KEY;
       vr[i] = (s + i < e) ? vals[s + i] : HMO_NOT_FOUND;
@@ -187,12 +188,11 @@ void hmo_search(const hmo_tree *t, const int64_t *q, int64_t n, int64_t *out) {
       continue;
     }
     int64_t leaf = descend(t, key);
-    const int64_t *row = t->leaf_keys + leaf * t->leaf_row;
+    const int64_t *row = t->leaf_rows + leaf * t->leaf_row;
     int r = rank_row(row, t->leaf_index, t->p.leaf_cap, key);
     const int64_t *kr = row + t->leaf_index;
     /* equality test of the matched slot, BLeaf_node::findKey (bpt.h:252-274) */
-    out[i] = (r > 0 && kr[r - 1] == key) ? t->leaf_vals[leaf * t->p.leaf_cap + r - 1]
-                                         : HMO_NOT_FOUND;
+    out[i] = (r > 0 && kr[r - 1] == key) ? kr[t->p.leaf_cap + r - 1] : HMO_NOT_FOUND;
   }
 }
 
@@ -205,7 +205,7 @@ int64_t hmo_range(const hmo_tree *t, const int64_t *start, const int32_t *len,
     int64_t want = len[i] > 0 ? len[i] : 0;
     if (want == 0 || start[i] == HMO_MAX_KEY) continue;
     int64_t leaf = descend(t, start[i]);
-    const int64_t *kr = t->leaf_keys + leaf * t->leaf_row + t->leaf_index;
+    const int64_t *kr = t->leaf_rows + leaf * t->leaf_row + t->leaf_index;
     int slot = 0; /* lower bound: first key >= start */
     while (slot < t->leaf_cnt[leaf] && kr[slot] < start[i]) slot++;
     int64_t got = 0;
@@ -216,8 +216,9 @@ int64_t hmo_range(const hmo_tree *t, const int64_t *start, const int32_t *len,
         continue;
       }
       if (total >= cap) return -1;
-      okeys[total] = t->leaf_keys[leaf * t->leaf_row + t->leaf_index + slot];
-      ovals[total] = t->leaf_vals[leaf * t->p.leaf_cap + slot];
+      const int64_t *r = t->leaf_rows + leaf * t->leaf_row + t->leaf_index;
+      okeys[total] = r[slot];
+      ovals[total] = r[t->p.leaf_cap + slot];
       total++;
       got++;
       slot++;
@@ -232,8 +233,9 @@ int64_t hmo_export(const hmo_tree *t, int64_t *keys, int64_t *vals, int64_t cap)
   int64_t o = 0;
   for (int64_t j = 0; j < t->n_leaf; j++)
     for (int s = 0; s < t->leaf_cnt[j]; s++) {
-      keys[o] = t->leaf_keys[j * t->leaf_row + t->leaf_index + s];
-      vals[o] = t->leaf_vals[j * t->p.leaf_cap + s];
+      const int64_t *r = t->leaf_rows + j * t->leaf_row + t->leaf_index;
+      keys[o] = r[s];
+      vals[o] = r[t->p.leaf_cap + s];
       o++;
     }
   return o;

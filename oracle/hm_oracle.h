@@ -42,14 +42,13 @@ typedef struct {
   hmo_params p;
   int height;       /* number of inner levels, >= 1 */
   int inner_row;    /* int64 words per inner row: F/8 index + F keys */
-  int leaf_row;     /* int64 words per leaf key row: (Lc>=32 ? Lc/8 : 0) index + Lc keys */
+  int leaf_row;     /* int64 words per leaf row: (Lc>=32 ? Lc/8 : 0) index, Lc keys, Lc values */
   int leaf_index;   /* index words at the start of a leaf row */
   int64_t n_keys, n_inner, n_leaf;
   int64_t lvl_start[HMO_MAX_LEVELS + 1]; /* BFS index of each inner level; lvl_start[height] = n_inner */
   int64_t *inner;     /* n_inner * inner_row */
   int32_t *prefix;    /* n_inner; children of the last level count from n_inner */
-  int64_t *leaf_keys; /* n_leaf * leaf_row */
-  int64_t *leaf_vals; /* n_leaf * Lc; -1 in empty slots */
+  int64_t *leaf_rows; /* n_leaf * leaf_row; keys Max_Key and values -1 in empty slots */
   int32_t *leaf_cnt;  /* n_leaf */
   int64_t *leaf_base; /* n_leaf, exclusive scan of leaf_cnt */
 } hmo_tree;

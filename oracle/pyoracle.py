@@ -51,7 +51,7 @@ class _Tree(ctypes.Structure):
                 ("leaf_row", ctypes.c_int), ("leaf_index", ctypes.c_int),
                 ("n_keys", _I64), ("n_inner", _I64), ("n_leaf", _I64),
                 ("lvl_start", _I64 * 33),
-                ("inner", _P), ("prefix", _P), ("leaf_keys", _P), ("leaf_vals", _P),
+                ("inner", _P), ("prefix", _P), ("leaf_rows", _P),
                 ("leaf_cnt", _P), ("leaf_base", _P)]
 
 
@@ -133,8 +133,7 @@ class PortTree:
             "n_leaf": t.n_leaf,
             "inner": self._arr(t.inner, t.n_inner * t.inner_row, ctypes.c_int64, np.int64),
             "prefix": self._arr(t.prefix, t.n_inner, ctypes.c_int32, np.int32),
-            "leaf_keys": self._arr(t.leaf_keys, t.n_leaf * t.leaf_row, ctypes.c_int64, np.int64),
-            "leaf_vals": self._arr(t.leaf_vals, t.n_leaf * t.p.leaf_cap, ctypes.c_int64, np.int64),
+            "leaf_rows": self._arr(t.leaf_rows, t.n_leaf * t.leaf_row, ctypes.c_int64, np.int64),
             "leaf_cnt": self._arr(t.leaf_cnt, t.n_leaf, ctypes.c_int32, np.int32),
             "leaf_base": self._arr(t.leaf_base, t.n_leaf, ctypes.c_int64, np.int64),
         }

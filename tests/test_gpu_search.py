@@ -41,7 +41,7 @@ def test_bulk_load_layout_bit_exact(n, fanout, leaf_cap):
         got = t.layout()
     for k in ("height", "lvl_start", "n_inner", "n_leaf"):
         assert got[k] == exp[k], k
-    for k in ("inner", "prefix", "leaf_keys", "leaf_vals", "leaf_cnt", "leaf_base"):
+    for k in ("inner", "prefix", "leaf_rows", "leaf_cnt", "leaf_base"):
         assert (got[k] == exp[k]).all(), k
 
 
@@ -52,7 +52,7 @@ def test_bulk_load_partial_fill_layout(inner_fill, leaf_fill):
     exp = po.PortTree(sk, dg.values_for(sk), 64, 16, inner_fill, leaf_fill).layout()
     with BPlusTree.bulk_load(keys, dg.values_for(keys), 64, 16, inner_fill, leaf_fill) as t:
         got = t.layout()
-    for k in ("inner", "prefix", "leaf_keys", "leaf_vals", "leaf_cnt", "leaf_base"):
+    for k in ("inner", "prefix", "leaf_rows", "leaf_cnt", "leaf_base"):
         assert (got[k] == exp[k]).all(), k
 
 
