@@ -180,20 +180,83 @@ def run_reference(args, ws, rank):
 
 
 def cpu_baseline_port(keys_sorted, vals_sorted, q, seconds: float = 10.0):
-    """The oracle's C restatement, single-threaded, on a bounded query sample."""
+    """The oracle's C restatement (OpenMP over the queries, as the reference's
+    search_cpu_test) on a bounded sample of the batch."""
     from oracle import pyoracle as po
 
     t = po.PortTree(keys_sorted, vals_sorted)
-    m = 1 << 16
+    m = 1 << 20
+    t.search(q[:m])  # warm
     a = time.perf_counter()
     done = 0
     while done < len(q) and time.perf_counter() - a < seconds:
         t.search(q[done:done + m])
         done += m
     sec = time.perf_counter() - a
-    return {"value": round(min(done, len(q)) / sec / 1e6, 3), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{min(done, len(q))} queries of the batch in {sec:.1f} s, scalar C restatement "
-                      f"(oracle/hm_oracle.c), 1 thread"}
+    cores = os.cpu_count() or 1
+    return {"value": round(min(done, len(q)) / sec / 1e6, 3), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{min(done, len(q))} queries of the batch in {sec:.1f} s, C restatement of the "
+                      f"search (oracle/hm_oracle.c), OpenMP over {cores} threads"}
+
+
+def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
+    """512 batches with sizes log-uniform in [1K, 4M], half uniform (90% hits),
+    half Zipf(0.99) over key rank: one plain launch per batch vs the whole set
+    in one captured CUDA graph (joint pre-sort + persistent search)."""
+    import torch
+    from harmonia_b200 import datagen as dg
+
+    nb = 512
+    r = dg.splitmix64(np.arange(nb, dtype=np.uint64) + np.uint64(seed) * np.uint64(1 << 40))
+    u = (r >> np.uint64(11)).astype(np.float64) / float(1 << 53)
+    sizes = np.exp(np.log(1024) + u * (np.log(4 << 20) - np.log(1024))).astype(np.int64)
+    pool_n = 1 << 24
+    pool_u = torch.from_numpy(dg.gen_point_queries(keys, pool_n, 0.9, seed + 1)).to(dev)
+    pool_z = torch.from_numpy(dg.gen_zipf_queries(sk, pool_n, 0.99, seed + 2)).to(dev)
+    total = int(sizes.sum())
+    allq = torch.empty(total, dtype=torch.int64, device=dev)
+    allo = torch.empty(total, dtype=torch.int64, device=dev)
+    batches, o = [], 0
+    for b in range(nb):
+        m = int(sizes[b])
+        pool = pool_u if b % 2 == 0 else pool_z
+        start = int(r[b] % np.uint64(pool_n))
+        idx = (torch.arange(m, device=dev) + start) % pool_n
+        allq[o:o + m] = pool[idx]
+        batches.append((allq[o:o + m], allo[o:o + m]))
+        o += m
+    del pool_u, pool_z
+    cfg = tree.config()
+    tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0)
+
+    def plain():
+        for q, out in batches:
+            tree.search(q, out)
+
+    for _ in range(warmup):
+        plain()
+    plain_ms = timed(steps, plain)
+    tree.set_search_config(**{k: cfg[k] for k in ("group_width", "queries_per_group", "sort_bits", "cache_hints")})
+    plan = tree.plan(batches)
+    for _ in range(warmup):
+        plan.launch()
+    plan_ms = timed(steps, plan.launch)
+    # spot check the last step's results of a few batches against the workload's own values
+    for b in (0, 1, nb // 2, nb - 1):
+        q, out = batches[b]
+        qq = q[:2048].cpu().numpy()
+        pos = np.searchsorted(sk, qq).clip(max=len(sk) - 1)
+        exp = np.where(sk[pos] == qq, dg.values_for(qq), -1)
+        assert (out[:2048].cpu().numpy() == exp).all(), "batched results are wrong"
+    plan.close()
+    return {"batches": nb, "queries": total, "min_batch": int(sizes.min()), "max_batch": int(sizes.max()),
+            "plain_per_batch": {"value": round(total / plain_ms / 1e3, 1), "unit": UNIT,
+                                "ms_per_step": round(plain_ms, 3),
+                                "what": "one search launch per batch, unsorted, group width 4, 2 queries/group"},
+            "graph": {"value": round(total / plan_ms / 1e3, 1), "unit": UNIT, "ms_per_step": round(plan_ms, 3),
+                      "what": "the 512 batches in one captured CUDA graph: gather, joint 16-bit pre-sort, "
+                              "persistent search, scatter back"},
+            "speedup": round(plain_ms / plan_ms, 3)}
 
 
 def main():
@@ -320,6 +383,10 @@ def main():
         tree.set_search_config(**{k: tuned[k] for k in ("group_width", "queries_per_group", "sort_bits",
                                                        "cache_hints")})
         del d_qs
+
+    if args.extras:
+        extras["batched_uneven"] = batched_uneven(tree, keys, sk, dev, timed, max(3, args.steps // 3),
+                                                  args.warmup)
 
     # ---- end to end through the public API with host (pinned) buffers ----
     h_q = torch.from_numpy(q).pin_memory()

@@ -17,7 +17,11 @@
 namespace hm {
 
 static std::atomic<uint64_t> g_launches{0};
-void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+static thread_local bool t_capturing = false;
+void note_launch(int n) {
+  if (!t_capturing) g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed);
+}
+void set_capturing(bool on) { t_capturing = on; }
 
 int cuda_err(cudaError_t e) {
   if (e == cudaSuccess) return HM_OK;
@@ -112,7 +116,7 @@ int check_config(const hm_config &c) {
   }
   if (c.queries_per_group != 1 && c.queries_per_group != 2 && c.queries_per_group != 4)
     return HM_EINVAL;
-  if (c.sort_bits < -1 || c.sort_bits > 12) return HM_EINVAL;
+  if (c.sort_bits < -1 || c.sort_bits > 16) return HM_EINVAL;
   if (c.smem_bytes < 0 || c.smem_bytes > 200 * 1024) return HM_EINVAL;
   if (c.cache_hints != 1 && c.cache_hints != 2) return HM_EINVAL;
   return HM_OK;
@@ -146,9 +150,9 @@ int sort_bits_for(const hm_tree *t, int64_t n) {
   if (n > INT32_MAX) return 0;  // positions are carried as int32
   int b = t->cfg.sort_bits;
   if (b >= 0) return b;
-  // auto: partition large batches only; 8 bits keeps >= 32 queries per
-  // bucket per partition CTA at the batch sizes where it pays.
-  return (n >= (1 << 21) && t->n_leaf >= (1 << 16)) ? 8 : 0;
+  // auto: pre-sort large batches on 16 bits (two stable passes); small
+  // batches cannot amortise the passes.
+  return (n >= (1 << 21) && t->n_leaf >= (1 << 16)) ? 16 : 0;
 }
 
 cudaStream_t as_stream(hm_stream s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -524,40 +528,6 @@ int hm_search(hm_tree *t, const int64_t *q, size_t n_, int64_t *out, hm_stream h
   return hm_sync(t, hs);
 }
 
-int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream hs) {
-  if (!t || nb < 0 || (nb > 0 && !batches)) return HM_EINVAL;
-  if (nb == 0) return HM_OK;
-  cudaStream_t s = as_stream(hs);
-  const int tileq = search_tile_queries(t->cfg.group_width, t->cfg.queries_per_group);
-  std::vector<int64_t> ts((size_t)nb + 2);
-  ts[0] = 0;
-  for (int i = 0; i < nb; i++) {
-    if (batches[i].n < 0 || (batches[i].n > 0 && (!batches[i].q || !batches[i].out)))
-      return HM_EINVAL;
-    ts[i + 1] = ts[i] + (batches[i].n + tileq - 1) / tileq;
-  }
-  ts[nb + 1] = 0;  // tile counter
-  size_t bbytes = align_up((int64_t)sizeof(hm_batch) * nb, 256);
-  size_t tbytes = align_up((int64_t)sizeof(int64_t) * (nb + 2), 256);
-  int rc = ensure_scratch(t, bbytes + tbytes);
-  if (rc) return rc;
-  char *sb = static_cast<char *>(t->scratch);
-  hm_batch *d_b = reinterpret_cast<hm_batch *>(sb);
-  int64_t *d_ts = reinterpret_cast<int64_t *>(sb + bbytes);
-  cudaError_t e = cudaMemcpyAsync(d_b, batches, sizeof(hm_batch) * nb, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_ts, ts.data(), sizeof(int64_t) * (nb + 2), cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return cuda_err(e);
-  // The host arrays must stay valid until the copies finish.
-  int tok = prof_begin(t, s);
-  rc = launch_search_batches(t, d_b, d_ts, nb, ts[nb], t->cfg.group_width,
-                             t->cfg.queries_per_group, s);
-  prof_end(t, kStageBatches, tok, s);
-  e = cudaStreamSynchronize(s);
-  if (rc) return rc;
-  return cuda_err(e);
-}
-
 int hm_sync(hm_tree *t, hm_stream hs) {
   if (!t) return HM_EINVAL;
   cudaError_t e = cudaStreamSynchronize(as_stream(hs));
@@ -722,7 +692,7 @@ int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n_, hm_config *best)
   float best_ms = 1e30f;
   const int widths[] = {2, 4, 8, 16, 32};
   const int qpgs[] = {1, 2, 4};
-  const int bits_list[] = {0, 6, 8, 10};
+  const int bits_list[] = {0, 8, 12, 16};
   const int hints_list[] = {1, 2};
   int rc = HM_OK;
   for (int w : widths)

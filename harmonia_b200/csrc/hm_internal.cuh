@@ -64,8 +64,10 @@ __host__ __device__ inline int64_t part_start(int64_t j, int64_t total, int64_t 
 
 inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
-// Counts kernel launches issued by this library (hm_launch_count).
+// Counts kernel launches issued by this library (hm_launch_count); launches
+// recorded into a CUDA graph are counted when the graph is replayed.
 void note_launch(int n = 1);
+void set_capturing(bool on);
 
 }  // namespace hm
 
@@ -80,6 +82,7 @@ struct hm_tree {
   int smem_nodes = 0;
   int num_sms = 148;
   int64_t key_min = 0, key_max = 0;  // for the pre-sort digit
+  uint64_t generation = 0;           // bumped when the arena is rebuilt
   // arena
   void *arena = nullptr;
   size_t arena_bytes = 0;
@@ -159,6 +162,9 @@ int launch_search_batches(const hm_tree *t, const hm_batch *d_batches, const int
                           int nb, int64_t total_tiles, int group_width, int qpg,
                           cudaStream_t s);
 int search_tile_queries(int group_width, int qpg);  // queries per CTA tile
+// Resolves (and caches) the kernel's launch configuration without launching,
+// so that a later launch can be captured in a CUDA graph.
+int launch_search_warm(const hm_tree *t, int group_width, int qpg);
 size_t search_smem_bytes(const hm_tree *t);
 
 // ---- query pre-sort (partition.cu) ----

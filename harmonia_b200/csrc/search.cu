@@ -423,6 +423,13 @@ size_t search_smem_bytes(const hm_tree *t) {
 
 int search_tile_queries(int group_width, int qpg) { return (kThreads / group_width) * qpg; }
 
+int launch_search_warm(const hm_tree *t, int group_width, int qpg) {
+  KernelFn fn = pick_kernel(group_width, t->cfg.fanout, t->cfg.leaf_cap, qpg);
+  if (!fn) return HM_EINVAL;
+  int blocks = 0;
+  return grid_for(t, fn, search_smem_bytes(t), &blocks);
+}
+
 int launch_search(const hm_tree *t, const SearchLaunch &l, int group_width, int qpg,
                   cudaStream_t s) {
   if (l.n <= 0) return HM_OK;

@@ -384,6 +384,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     t->n_inner = nt.n_inner;
     t->n_leaf = nt.n_leaf;
     t->n_keys = n1;
+    t->generation++;
   }
   if (t->n_keys == nm || new_ends[0] < t->key_min) t->key_min = new_ends[0];
   if (t->n_keys == nm || new_ends[1] > t->key_max) t->key_max = new_ends[1];

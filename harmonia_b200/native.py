@@ -25,7 +25,7 @@ EXPORTS = (
     "hm_config_default", "hm_bulk_load", "hm_search", "hm_search_batches", "hm_range",
     "hm_upsert_batch", "hm_export", "hm_tree_get_info", "hm_set_search_config",
     "hm_get_config", "hm_autotune", "hm_sync", "hm_free", "hm_strerror", "hm_launch_count",
-    "hm_profile", "hm_profile_read",
+    "hm_profile", "hm_profile_read", "hm_plan_create", "hm_plan_launch", "hm_plan_free",
 )
 
 
@@ -99,6 +99,9 @@ def lib() -> ctypes.CDLL:
     L.hm_launch_count.argtypes = []
     L.hm_launch_count.restype = ctypes.c_uint64
     L.hm_profile.argtypes = [P, I]
+    L.hm_plan_create.argtypes = [P, ctypes.POINTER(Batch), I, PT]
+    L.hm_plan_launch.argtypes = [P, P]
+    L.hm_plan_free.argtypes = [P]
     L.hm_profile_read.argtypes = [P, ctypes.POINTER(StageTime), I, ctypes.POINTER(I)]
     _lib = L
     return L

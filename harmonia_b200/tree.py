@@ -141,6 +141,10 @@ class BPlusTree:
             arr[i].n = len(q)
         check(lib().hm_search_batches(self._h, arr, len(batches), _stream_ptr(stream)), "hm_search_batches")
 
+    def plan(self, batches) -> "Plan":
+        """Captures a CUDA graph searching these (queries, out) CUDA tensor pairs."""
+        return Plan(self, batches)
+
     def range_search(self, start, length, stream=None):
         """Returns (offsets[n+1], keys, values): query i owns [offsets[i], offsets[i+1])."""
         start = _as_i64(start)
@@ -248,6 +252,36 @@ class BPlusTree:
             "leaf_cnt": grab(i.leaf_cnt, i.n_leaf, 4, np.int32),
             "leaf_base": grab(i.leaf_base, i.n_leaf, 8, np.int64),
         }
+
+
+class Plan:
+    """A batch set captured as a CUDA graph (hm_plan); launch() replays it."""
+
+    def __init__(self, tree: BPlusTree, batches):
+        self._tree = tree  # keeps the tree alive while the plan exists
+        self._bufs = list(batches)
+        arr = (native.Batch * max(len(batches), 1))()
+        for i, (q, o) in enumerate(batches):
+            arr[i].q = _ptr(q)
+            arr[i].out = _ptr(o)
+            arr[i].n = len(q)
+        h = ctypes.c_void_p()
+        check(lib().hm_plan_create(tree.handle, arr, len(batches), ctypes.byref(h)), "hm_plan_create")
+        self._h = h
+
+    def launch(self, stream=None) -> None:
+        check(lib().hm_plan_launch(self._h, _stream_ptr(stream)), "hm_plan_launch")
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            check(lib().hm_plan_free(self._h), "hm_plan_free")
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def launch_count() -> int:

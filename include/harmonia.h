@@ -67,7 +67,7 @@ typedef struct {
   int leaf_fill;         /* keys per leaf at bulk load, 1..leaf_cap (default leaf_cap) */
   int group_width;       /* lanes cooperating on one query: 1,2,4,8,16,32 (default 4) */
   int queries_per_group; /* queries a group keeps in flight: 1,2,4 (default 2) */
-  int sort_bits;         /* query pre-sort: top bits partitioned, 0 = off, -1 = auto (default -1) */
+  int sort_bits;         /* query pre-sort: top bits, 0 = off, 1..16, -1 = auto (default -1) */
   int smem_bytes;        /* budget for top levels staged in shared memory (default 49152) */
   int cache_hints;       /* L2 policy: 1 = inner rows evict_last, leaves evict_first; 2 = none
                             (default 1) */
@@ -119,10 +119,23 @@ typedef struct {
   int64_t n;
 } hm_batch;
 
-/* Searches nb independent batches (device buffers) in one persistent kernel.
+/* Searches nb independent batches (device buffers) together: small sets in
+ * one persistent kernel that hands out tiles of all batches, large sets
+ * gathered, pre-sorted together, searched and scattered back.  Returns when
+ * done.
  * Replaces: the per-bucket launch loop of launch_kernel_thread,
  * open-harmonia/src/full-multi-prefix-sort-8thread.cu:276-327. */
 int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream s);
+
+/* A batch set captured once as a CUDA graph and replayed: the batch buffers
+ * are fixed, their contents may change between launches.  The plan owns its
+ * work memory; it re-captures itself after the tree is rebuilt or retuned.
+ * hm_plan_launch only enqueues on s.  (No reference counterpart: the
+ * reference re-issues every launch from its launcher thread.) */
+typedef struct hm_plan hm_plan;
+int hm_plan_create(hm_tree *t, const hm_batch *batches, int nb, hm_plan **out);
+int hm_plan_launch(hm_plan *p, hm_stream s);
+int hm_plan_free(hm_plan *p);
 
 /* Range scan: for query i the first len[i] records with key >= start[i], in
  * key order (fewer if the key space ends), compacted: query i's records are

@@ -181,6 +181,9 @@ static int64_t descend(const hmo_tree *t, int64_t q) {
 }
 
 void hmo_search(const hmo_tree *t, const int64_t *q, int64_t n, int64_t *out) {
+  /* one query per iteration, like search_cpu_test's OpenMP loop
+   * (open-harmonia/src/main.cpp:795-799) */
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; i++) {
     int64_t key = q[i];
     if (key == HMO_MAX_KEY) { /* no stored key equals the sentinel */

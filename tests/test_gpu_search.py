@@ -84,7 +84,7 @@ def test_every_group_width_and_depth(c1, w, qpg):
         t.set_search_config(group_width=4, queries_per_group=2, sort_bits=-1)
 
 
-@pytest.mark.parametrize("bits", [1, 4, 8, 12])
+@pytest.mark.parametrize("bits", [1, 4, 8, 9, 12, 16])
 def test_presort_bits(c1, bits):
     keys, sk, t = c1
     q = dg.gen_point_queries(keys, 1 << 19, 0.9, seed=bits)
@@ -183,3 +183,50 @@ def test_launches_come_from_the_library(c1):
     t.search(cuda(keys[:1000]))
     torch.cuda.synchronize()
     assert native.lib().hm_launch_count() > before
+
+
+def test_search_batches_large_presorted_union(c1):
+    """Large sets take the gather / joint pre-sort / scatter-back path."""
+    keys, sk, t = c1
+    oracle = po.PortTree(sk, dg.values_for(sk))
+    sizes = [1 << 20, 1000, 1 << 19, 5, 777777]
+    qs = [dg.gen_point_queries(keys, m, 0.6, seed=400 + i) for i, m in enumerate(sizes)]
+    outs = [torch.full((len(q),), -77, dtype=torch.int64, device="cuda") for q in qs]
+    for bits in (16, 8, 0):
+        t.set_search_config(sort_bits=bits)
+        for o in outs:
+            o.fill_(-77)
+        t.search_batches(list(zip([cuda(q) for q in qs], outs)))
+        for q, o in zip(qs, outs):
+            assert (o.cpu().numpy() == oracle.search(q)).all(), bits
+    t.set_search_config(sort_bits=-1)
+
+
+def test_plan_replay_matches_and_follows_rebuild():
+    keys = dg.gen_keys(1 << 18, seed=61)
+    vals = dg.values_for(keys)
+    sk = np.sort(keys)
+    with BPlusTree.bulk_load(cuda(keys), cuda(vals)) as t:
+        sizes = [3 << 20, 4096, 1, 100000]
+        qs = [cuda(dg.gen_point_queries(keys, m, 0.5, seed=70 + i)) for i, m in enumerate(sizes)]
+        outs = [torch.empty_like(q) for q in qs]
+        plan = t.plan(list(zip(qs, outs)))
+        for rep in range(3):
+            for q in qs:  # new contents in the same buffers
+                q.copy_(cuda(dg.gen_point_queries(keys, len(q), 0.5, seed=80 + rep + len(q))))
+            plan.launch()
+            torch.cuda.synchronize()
+            exp = po.PortTree(sk, dg.values_for(sk))
+            for q, o in zip(qs, outs):
+                assert (o.cpu().numpy() == exp.search(q.cpu().numpy())).all()
+        # a rebuild (overflowing upsert) moves the arena: the plan re-captures itself
+        bk, bv = dg.gen_upserts(keys, 300000, 1.0, seed=90)
+        t.upsert(bk, bv)
+        ek, ev = po.upsert_set(sk, dg.values_for(sk), bk, bv)
+        t.set_search_config(group_width=8)
+        plan.launch()
+        torch.cuda.synchronize()
+        exp = po.PortTree(ek, ev)
+        for q, o in zip(qs, outs):
+            assert (o.cpu().numpy() == exp.search(q.cpu().numpy())).all()
+        plan.close()
