@@ -26,7 +26,9 @@ EXPORTS = (
     "hm_upsert_batch", "hm_export", "hm_tree_get_info", "hm_set_search_config",
     "hm_get_config", "hm_autotune", "hm_sync", "hm_free", "hm_strerror", "hm_launch_count",
     "hm_profile", "hm_profile_read", "hm_plan_create", "hm_plan_launch", "hm_plan_free",
+    "hm_search_noalloc",
 )
+HM_NOALLOC_MAX_QUERIES = 1 << 20
 
 
 class HarmoniaError(RuntimeError):
@@ -102,6 +104,7 @@ def lib() -> ctypes.CDLL:
     L.hm_plan_create.argtypes = [P, ctypes.POINTER(Batch), I, PT]
     L.hm_plan_launch.argtypes = [P, P]
     L.hm_plan_free.argtypes = [P]
+    L.hm_search_noalloc.argtypes = [P, P, SZ, P, P]
     L.hm_profile_read.argtypes = [P, ctypes.POINTER(StageTime), I, ctypes.POINTER(I)]
     _lib = L
     return L

@@ -188,6 +188,24 @@ int hm_sync(hm_tree *t, hm_stream s);
 int hm_free(hm_tree *t);
 const char *hm_strerror(int code);
 
+/* Point search that allocates nothing, for callers that cannot allocate
+ * device memory when they search: code running while a CUDA graph is being
+ * captured, a serving loop held to a fixed memory budget, or a host runtime
+ * that owns all device memory and hands the library only its buffers.  It
+ * runs the same pre-sort (8 bits) and search as hm_search, with its working
+ * space in one fixed array the library keeps in device memory
+ * (HM_NOALLOC_SCRATCH_BYTES on every GPU that loads the library, held until
+ * the process exits).  q and out must be device memory, n at most
+ * HM_NOALLOC_MAX_QUERIES (HM_ETOOLARGE otherwise, HM_EINVAL for host
+ * buffers).  Only enqueues on s.  The first call on a device looks the
+ * array's address up; make it before any stream capture.  All calls on a
+ * device share the array: calls that overlap on the GPU race, so serialise
+ * them.  No counterpart in the reference, whose drivers cudaMalloc their
+ * buffers per experiment (open-harmonia/src/full-multi-prefix-sort-8thread.cu:409-433). */
+#define HM_NOALLOC_MAX_QUERIES (1 << 20)
+#define HM_NOALLOC_SCRATCH_BYTES (14u << 20)
+int hm_search_noalloc(hm_tree *t, const int64_t *q, size_t n, int64_t *out, hm_stream s);
+
 /* Kernel launches this library has issued since load (for launch counting). */
 uint64_t hm_launch_count(void);
 
