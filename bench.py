@@ -259,6 +259,87 @@ def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
             "speedup": round(plain_ms / plan_ms, 3)}
 
 
+def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
+    """Serving workload: a 2^25-key tree; Poisson arrivals, request sizes
+    log-uniform in [64, 2^20]; 90% point search (80% hits), 5% range (length
+    1..128), 5% upsert (half new, half existing keys) applied in epochs.
+    Offered loads are fractions of the measured capacity of back-to-back
+    point requests; reports throughput and p50/p99 submit-to-completion
+    latency at each load, and checks a sample of answers."""
+    import threading
+    from harmonia_b200 import BPlusTree, datagen as dg
+    from harmonia_b200.serving import Server
+
+    n = 1 << 25
+    keys = dg.gen_keys(n, seed)
+    tree = BPlusTree.bulk_load(keys, dg.values_for(keys), leaf_fill=12)
+    pool = dg.gen_point_queries(keys, 1 << 24, 0.8, seed + 1)
+    rstart, rlen = dg.gen_ranges(1 << 16, 1, 128, seed + 2)
+    rng = np.random.default_rng(seed)
+    out = {}
+    with Server(tree, streams=3, max_launch_queries=1 << 22, device_budget_bytes=2 << 30) as srv:
+        def sizes(k):
+            return np.exp(rng.uniform(np.log(64), np.log(1 << 20), k)).astype(np.int64)
+        # capacity: back-to-back point requests of the same size law
+        cap_sizes = sizes(200)
+        offs = rng.integers(0, len(pool) - (1 << 20), 200)
+        t0 = time.perf_counter()
+        tks = [srv.search(pool[o:o + m]) for o, m in zip(offs, cap_sizes)]
+        for tk in tks:
+            tk.wait()
+        cap_qps = cap_sizes.sum() / (time.perf_counter() - t0)
+        mean_size = float(np.exp(np.log(1 << 20) - np.log(64)) - 1) * 64 / np.log((1 << 20) / 64)
+        for frac in loads:
+            rate = frac * cap_qps / mean_size  # requests per second
+            srv.reset_stats()
+            count = int(rate * seconds) + 1
+            gaps = rng.exponential(1.0 / rate, count)
+            kinds = rng.random(count)
+            szs = sizes(count)
+            tickets = []
+            t_start = time.perf_counter()
+            due = t_start
+            new_keys = dg.gen_keys(count * 64, seed + 100 + int(frac * 100))
+            for i in range(count):
+                due += gaps[i]
+                while time.perf_counter() < due:
+                    pass
+                m = int(szs[i])
+                if kinds[i] < 0.90:
+                    o = int(rng.integers(0, len(pool) - m))
+                    tickets.append(("s", srv.search(pool[o:o + m]), o, m))
+                elif kinds[i] < 0.95:
+                    k = max(1, m // 64)
+                    o = int(rng.integers(0, len(rstart) - k))
+                    tickets.append(("r", srv.range(rstart[o:o + k], rlen[o:o + k]), o, k))
+                else:
+                    k = max(2, min(m // 16, 64))
+                    nk = new_keys[i * 64:i * 64 + k // 2]
+                    ek = keys[rng.integers(0, n, k - k // 2)]
+                    bk = np.concatenate([nk, ek])
+                    bv = np.concatenate([dg.values_for(nk), ek - 1])
+                    tickets.append(("u", srv.upsert(bk, bv), 0, k))
+            for kind, tk, o, m in tickets:
+                tk.wait()
+            wall = time.perf_counter() - t_start
+            st = srv.stats()
+            out[f"load_{frac}"] = {"offered_req_per_s": round(rate, 1), "requests": count,
+                                   "throughput_mqps": round(st["queries"] / wall / 1e6, 1),
+                                   "p50_ms": round(st["p50_us"] / 1e3, 3), "p99_ms": round(st["p99_us"] / 1e3, 3),
+                                   "max_ms": round(st["max_us"] / 1e3, 3), "launches": st["launches"],
+                                   "epochs": st["epochs"], "failed": st["failed"]}
+        # answers in the mix: a point request's hits return splitmix64(key)>>1 or key-1 (updated)
+        s_hits = [t for t in tickets if t[0] == "s"][:20]
+        for kind, tk, o, m in s_hits:
+            q = pool[o:o + m]
+            got = tk._result()
+            ok = (got == -1) | (got == dg.values_for(q)) | (got == q - 1)
+            assert ok.all(), "serving answer outside the possible values"
+        out["capacity_mqps"] = round(cap_qps / 1e6, 1)
+    tree.close()
+    return out
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -271,6 +352,7 @@ def main():
     import torch.distributed as dist
 
     from harmonia_b200 import BPlusTree, datagen as dg, launch_count
+    from harmonia_b200 import replicas
 
     torch.cuda.set_device(local)
     if ws > 1:
@@ -282,7 +364,7 @@ def main():
     m = 1 << args.queries_log2
     keys = dg.gen_keys(n, 1)
     vals = dg.values_for(keys)
-    q = dg.gen_point_queries(keys, m, args.hit, 2 + 1000 * rank)
+    q = dg.gen_point_queries(keys, m, args.hit, replicas.query_seed(2, rank))
     d_keys = torch.from_numpy(keys).to(dev)
     d_vals = torch.from_numpy(vals).to(dev)
     torch.cuda.synchronize()
@@ -309,11 +391,7 @@ def main():
         torch.cuda.synchronize()
         if ws > 1:
             dist.barrier()
-        ms = a.elapsed_time(b)
-        if ws > 1:
-            x = torch.tensor([ms], device=dev)
-            dist.all_reduce(x, op=dist.ReduceOp.MAX)
-            ms = float(x.item())
+        ms = replicas.max_over_ranks(a.elapsed_time(b), dev if ws > 1 else None)
         return ms / steps
 
     extras = {}
@@ -350,7 +428,7 @@ def main():
     launches = launch_count() - l0
     stages = tree.profile_read()
     tree.profile(False)
-    value = ws * m / ms / 1e3  # Mqueries/s (m queries per rank per step)
+    value = replicas.job_throughput(m, ws, ms)  # Mqueries/s (m queries per rank per step)
 
     search_launches, search_total = stages.get("search", (0, 0.0))
     search_ms = search_total / max(search_launches, 1)
@@ -398,6 +476,9 @@ def main():
     e2e = {"value": round(ws * m / e2e_ms / 1e3, 1), "unit": UNIT, "h2d_bytes_per_step": m * 8,
            "d2h_bytes_per_step": m * 8, "ms_per_step": round(e2e_ms, 3),
            "what": "BPlusTree.search on pinned host buffers: chunked H2D, search, D2H through the C ABI"}
+
+    if args.extras and rank == 0:
+        extras["serving"] = serving_loads(dev)
 
     cpu = None
     if rank == 0 and ws == 1:

@@ -23,8 +23,11 @@ void note_launch(int n) {
 }
 void set_capturing(bool on) { t_capturing = on; }
 
+static std::atomic<int> g_last_cuda{0};
+
 int cuda_err(cudaError_t e) {
   if (e == cudaSuccess) return HM_OK;
+  g_last_cuda.store((int)e);
   if (e == cudaErrorMemoryAllocation) return HM_ENOMEM;
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return HM_ENODEVICE;
   return HM_ECUDA;
@@ -240,6 +243,16 @@ size_t search_scratch_need(const hm_tree *t, int64_t n) {
 
 }  // namespace
 
+namespace hm {
+// Entry points into this file's helpers for the other host sources.
+int run_search(hm_tree *t, const int64_t *d_q, int64_t n, int64_t *d_out, cudaStream_t s,
+               void *scratch, size_t scratch_bytes) {
+  return search_device(t, d_q, n, d_out, s, scratch, scratch_bytes);
+}
+size_t run_search_scratch(const hm_tree *t, int64_t n) { return search_scratch_need(t, n); }
+void refresh_smem_levels(hm_tree *t) { choose_smem_levels(t); }
+}  // namespace hm
+
 extern "C" {
 
 int hm_config_default(hm_config *cfg) {
@@ -269,6 +282,14 @@ const char *hm_strerror(int code) {
 }
 
 uint64_t hm_launch_count(void) { return g_launches.load(); }
+
+int hm_last_cuda_error(char *buf, size_t cap) {
+  const int e = g_last_cuda.load();
+  if (buf && cap > 0) {
+    std::snprintf(buf, cap, "%s: %s", cudaGetErrorName((cudaError_t)e), cudaGetErrorString((cudaError_t)e));
+  }
+  return e;
+}
 
 int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_config *cfg_in,
                  hm_tree **out) {

@@ -195,6 +195,14 @@ enum Stage { kStagePartition = 0, kStageSearch, kStageBatches, kStageRange, kSta
 int prof_begin(hm_tree *t, cudaStream_t s);
 void prof_end(hm_tree *t, int stage, int token, cudaStream_t s);
 
+// ---- host helpers (harmonia.cu) ----
+// Point search of device-resident queries on s, with the configured pre-sort;
+// scratch must hold run_search_scratch(t, n) bytes.
+int run_search(hm_tree *t, const int64_t *d_q, int64_t n, int64_t *d_out, cudaStream_t s,
+               void *scratch, size_t scratch_bytes);
+size_t run_search_scratch(const hm_tree *t, int64_t n);
+void refresh_smem_levels(hm_tree *t);
+
 // ---- misc ----
 int ensure_scratch(hm_tree *t, size_t bytes);
 int cuda_err(cudaError_t e);

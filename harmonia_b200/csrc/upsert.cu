@@ -233,7 +233,11 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   // scratch: uk, uk_alt, idx, idx_alt (n each, 8 B), keep/miss/leaf_of/is_start (4 B),
   // at (8 B, n+1), bk, bv, mk, mv, run_start (8 B), run_len/run_leaf/ml (4 B), sort scratch, flags
   const size_t s8 = al(8 * (n + 1)), s4 = al(4 * (n + 1));
-  size_t need = 9 * s8 + 7 * s4 + al((int64_t)radix_scratch_bytes(n)) + al((int64_t)scan_scratch_bytes(n + 1)) + 256;
+  // the leaf_base rescan covers every leaf, not just the batch
+  const int64_t scan_n = std::max<int64_t>(n, t->n_leaf) + 1;
+  const size_t lb8 = al(8 * (t->n_leaf + 1));
+  size_t need = 9 * s8 + 7 * s4 + lb8 + al((int64_t)radix_scratch_bytes(n)) +
+                al((int64_t)scan_scratch_bytes(scan_n)) + 256;
   int rc = ensure_scratch(t, need);
   if (rc) return rc;
   char *p = static_cast<char *>(t->scratch);
@@ -258,8 +262,10 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   int64_t *run_start = idx_alt;  // free once the sort is done
   void *sort_scratch = p;
   p += al((int64_t)radix_scratch_bytes(n));
+  int64_t *lbase_tmp = reinterpret_cast<int64_t *>(p);  // n_leaf + 1 entries
+  p += lb8;
   void *scan_scratch = p;
-  p += al((int64_t)scan_scratch_bytes(n + 1));
+  p += al((int64_t)scan_scratch_bytes(scan_n));
   unsigned *dflags = reinterpret_cast<unsigned *>(p);
 
   cudaMemsetAsync(dflags, 0, 8, s);
@@ -313,8 +319,8 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     merge_leaf_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(t->leaf_rows, t->leaf_cnt, lc,
                                                             li, mk, mv, is_start, run_start, run_len,
                                                             run_leaf, nm);
-    exclusive_scan_i32(t->leaf_cnt, at, t->n_leaf, scan_scratch, s);
-    cudaMemcpyAsync(t->leaf_base, at, 8 * t->n_leaf, cudaMemcpyDeviceToDevice, s);
+    exclusive_scan_i32(t->leaf_cnt, lbase_tmp, t->n_leaf, scan_scratch, s);
+    cudaMemcpyAsync(t->leaf_base, lbase_tmp, 8 * t->n_leaf, cudaMemcpyDeviceToDevice, s);
     note_launch();
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_err(e);

@@ -26,7 +26,9 @@ EXPORTS = (
     "hm_upsert_batch", "hm_export", "hm_tree_get_info", "hm_set_search_config",
     "hm_get_config", "hm_autotune", "hm_sync", "hm_free", "hm_strerror", "hm_launch_count",
     "hm_profile", "hm_profile_read", "hm_plan_create", "hm_plan_launch", "hm_plan_free",
-    "hm_search_noalloc",
+    "hm_search_noalloc", "hm_server_config_default", "hm_server_start", "hm_server_submit",
+    "hm_server_wait", "hm_server_get_stats", "hm_server_reset_stats", "hm_server_stop", "hm_server_free",
+    "hm_last_cuda_error",
 )
 HM_NOALLOC_MAX_QUERIES = 1 << 20
 
@@ -36,6 +38,10 @@ class HarmoniaError(RuntimeError):
         self.code = code
         name = ERRORS.get(code, str(code))
         msg = _lib.hm_strerror(code).decode() if _lib is not None else name
+        if _lib is not None and code in (-2, -5, -8):
+            buf = ctypes.create_string_buffer(256)
+            if _lib.hm_last_cuda_error(buf, 256):
+                msg += "; " + buf.value.decode()
         super().__init__(f"{what}: {name} ({msg})" if what else f"{name} ({msg})")
 
 
@@ -100,6 +106,7 @@ def lib() -> ctypes.CDLL:
     L.hm_strerror.restype = ctypes.c_char_p
     L.hm_launch_count.argtypes = []
     L.hm_launch_count.restype = ctypes.c_uint64
+    L.hm_last_cuda_error.argtypes = [ctypes.c_char_p, SZ]
     L.hm_profile.argtypes = [P, I]
     L.hm_plan_create.argtypes = [P, ctypes.POINTER(Batch), I, PT]
     L.hm_plan_launch.argtypes = [P, P]

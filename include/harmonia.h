@@ -188,6 +188,65 @@ int hm_sync(hm_tree *t, hm_stream s);
 int hm_free(hm_tree *t);
 const char *hm_strerror(int code);
 
+/* ---- Serving loop ----
+ * A request queue in front of one tree.  Callers submit point-search, range
+ * and upsert requests with host buffers and wait on the returned ticket.  A
+ * dispatcher thread admits requests in submission order while their device
+ * bytes fit the budget, coalesces consecutive reads of one kind into one
+ * launch, and keeps up to `streams` launches in flight (requests arriving
+ * while others run are admitted as slots and memory free up).  An upsert is
+ * an epoch barrier: it applies after every earlier request and before every
+ * later one, so a read returns what it would return alone against the
+ * upserts submitted before it.  Every device wait is bounded
+ * (device_wait_limit_ms).  No counterpart in the reference, which only runs
+ * offline experiments (open-harmonia/src/main.cpp:160-417). */
+enum { HM_REQ_SEARCH = 0, HM_REQ_RANGE = 1, HM_REQ_UPSERT = 2 };
+
+typedef struct {
+  int kind;              /* HM_REQ_* */
+  const int64_t *keys;   /* search: queries; range: start keys; upsert: keys (host) */
+  const int32_t *lens;   /* range: record counts */
+  const int64_t *vals;   /* upsert: values */
+  size_t n;
+  int64_t *out;          /* search: n values or -1 */
+  int64_t *offsets;      /* range: n+1 offsets into out_keys/out_vals */
+  int64_t *out_keys, *out_vals;
+  size_t out_cap;        /* range: record capacity; HM_ECAPACITY if exceeded */
+  int flags;             /* upsert: HM_UPSERT_* */
+} hm_request;
+
+typedef struct {
+  size_t device_budget_bytes;  /* device bytes of admitted, unfinished requests (default 1 GiB) */
+  int max_queue;               /* pending requests before HM_EBUSY (default 65536) */
+  int streams;                 /* launches in flight (default 3) */
+  int64_t max_launch_queries;  /* coalescing cap per launch (default 2^22) */
+  int64_t device_wait_limit_ms; /* a launch unfinished after this fails with HM_ETIMEOUT (default 30000) */
+} hm_server_config;
+
+typedef struct {
+  uint64_t completed, failed, rejected, launches, epochs, queries, pending;
+  double p50_us, p99_us, max_us, mean_us; /* submit-to-completion latency */
+  double elapsed_s;
+} hm_server_stats;
+
+typedef struct hm_server hm_server;
+int hm_server_config_default(hm_server_config *cfg);
+int hm_server_start(hm_tree *t, const hm_server_config *cfg, hm_server **out);
+/* Copies the request descriptor (not the buffers, which must stay valid until
+ * the request completes).  HM_EBUSY when the queue is full or the request
+ * alone exceeds the budget; HM_ECANCELLED after stop. */
+int hm_server_submit(hm_server *sv, const hm_request *r, uint64_t *ticket);
+/* Waits up to timeout_us (< 0: no limit) for the ticket; *status receives the
+ * request's HM_* result.  Returns HM_ETIMEOUT if still running. */
+int hm_server_wait(hm_server *sv, uint64_t ticket, int64_t timeout_us, int *status);
+int hm_server_get_stats(hm_server *sv, hm_server_stats *st);
+int hm_server_reset_stats(hm_server *sv);
+/* Cancels queued requests (their status becomes HM_ECANCELLED), lets those in
+ * flight finish and joins the dispatcher; tickets can still be waited on. */
+int hm_server_stop(hm_server *sv);
+/* Stops if needed and frees the server and every uncollected request. */
+int hm_server_free(hm_server *sv);
+
 /* Point search that allocates nothing, for callers that cannot allocate
  * device memory when they search: code running while a CUDA graph is being
  * captured, a serving loop held to a fixed memory budget, or a host runtime
@@ -205,6 +264,11 @@ const char *hm_strerror(int code);
 #define HM_NOALLOC_MAX_QUERIES (1 << 20)
 #define HM_NOALLOC_SCRATCH_BYTES (14u << 20)
 int hm_search_noalloc(hm_tree *t, const int64_t *q, size_t n, int64_t *out, hm_stream s);
+
+/* The last CUDA runtime error any call of this library turned into HM_ECUDA,
+ * HM_ENOMEM or HM_ENODEVICE (0 if none); its name and description go to buf.
+ * Replaces: the printf of CUDA_ERROR_HANDLER (open-harmonia/src/cuda_utils.h:3-12). */
+int hm_last_cuda_error(char *buf, size_t cap);
 
 /* Kernel launches this library has issued since load (for launch counting). */
 uint64_t hm_launch_count(void);

@@ -98,3 +98,21 @@ def test_many_small_epochs_stay_exact():
             sk, sv = po.upsert_set(sk, sv, bk, bv)
         xk, xv = t.export()
         assert (xk == sk).all() and (xv == sv).all()
+
+
+def test_tiny_batches_on_a_large_tree():
+    """In-place epochs of a few keys on a tree with far more leaves than keys
+    in the batch (the rescan of leaf_base spans all leaves)."""
+    keys = dg.gen_keys(1 << 21, seed=71)
+    sk, sv = np.sort(keys), dg.values_for(np.sort(keys))
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), leaf_fill=12) as t:
+        for e, m in enumerate((1, 3, 10, 64, 2)):
+            bk, bv = dg.gen_upserts(sk, m, 0.5, seed=700 + e)
+            t.upsert(bk, bv)
+            sk, sv = po.upsert_set(sk, sv, bk, bv)
+        xk, xv = t.export()
+        assert (xk == sk).all() and (xv == sv).all()
+        st, ln = dg.gen_ranges(2000, 1, 128, seed=77)
+        got = t.range_search(st, ln)
+        exp = po.PortTree(sk, sv).range(st, ln)
+        assert all((a == b).all() for a, b in zip(got, exp))
