@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--qpg", type=int, default=2)
     ap.add_argument("--sort-bits", type=int, default=-1)
     ap.add_argument("--hints", type=int, default=1)
+    ap.add_argument("--join", type=int, default=-1, help="1 bucket join, 2 never, -1 auto")
     ap.add_argument("--cpu-sample-log2", type=int, default=22)
     ap.add_argument("--extras", type=int, default=1, help="also time plain / pre-sorted input / e2e")
     return ap.parse_args()
@@ -227,7 +228,7 @@ def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
         o += m
     del pool_u, pool_z
     cfg = tree.config()
-    tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0)
+    tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0, join=2)
 
     def plain():
         for q, out in batches:
@@ -236,7 +237,8 @@ def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
     for _ in range(warmup):
         plain()
     plain_ms = timed(steps, plain)
-    tree.set_search_config(**{k: cfg[k] for k in ("group_width", "queries_per_group", "sort_bits", "cache_hints")})
+    tree.set_search_config(**{k: cfg[k] for k in ("group_width", "queries_per_group", "sort_bits", "cache_hints",
+                                                   "join")})
     plan = tree.plan(batches)
     for _ in range(warmup):
         plan.launch()
@@ -397,7 +399,7 @@ def main():
     extras = {}
     # plain single-batch launch: unsorted, default group width/depth, no tuning
     if args.extras:
-        tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0)
+        tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0, join=2)
         for _ in range(args.warmup):
             tree.search(d_q, d_out)
         plain_ms = timed(args.steps, lambda: tree.search(d_q, d_out))
@@ -405,7 +407,7 @@ def main():
                            "what": "one launch of the search kernel on the unsorted batch, group width 4, "
                                    "2 queries per group, no pre-sort"}
     tree.set_search_config(group_width=args.group_width, queries_per_group=args.qpg,
-                           sort_bits=args.sort_bits, cache_hints=args.hints)
+                           sort_bits=args.sort_bits, cache_hints=args.hints, join=args.join)
     tuned = tree.config()
     if not args.no_tune:
         tuned = tree.autotune(d_q)
@@ -439,7 +441,8 @@ def main():
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(f"search_f{args.fanout}_lc{args.leaf_cap}_bits{tuned['sort_bits']}")
+            key = "join" if stages.get("join") else f"bits{tuned['sort_bits']}"
+            traffic = json.load(open(tf)).get(f"search_f{args.fanout}_lc{args.leaf_cap}_{key}")
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "kernel": "search_kernel", "achieved": round(achieved, 1) if achieved else None,
@@ -452,14 +455,14 @@ def main():
     if args.extras:
         order = np.argsort(q >> np.int64(47), kind="stable")
         d_qs = torch.from_numpy(q[order]).to(dev)
-        tree.set_search_config(sort_bits=0)
+        tree.set_search_config(sort_bits=0, join=2)
         for _ in range(args.warmup):
             tree.search(d_qs, d_out)
         ps_ms = timed(args.steps, lambda: tree.search(d_qs, d_out))
         extras["presorted_input"] = {"value": round(ws * m / ps_ms / 1e3, 1), "unit": UNIT,
                                      "what": "batch pre-sorted by its top 16 key bits before the timed region"}
         tree.set_search_config(**{k: tuned[k] for k in ("group_width", "queries_per_group", "sort_bits",
-                                                       "cache_hints")})
+                                                       "cache_hints", "join")})
         del d_qs
 
     if args.extras:
@@ -497,7 +500,7 @@ def main():
                              f"{info.device_bytes / 2**30:.2f} GiB), no flush",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                        "tuned": {k: tuned[k] for k in ("group_width", "queries_per_group", "sort_bits",
-                                                       "cache_hints")},
+                                                       "cache_hints", "join")},
                        "tree": {"height": info.height, "n_inner": info.n_inner, "n_leaf": info.n_leaf,
                                 "smem_levels": info.smem_levels},
                        "bulk_load_ms": round(bulk_ms, 1)},

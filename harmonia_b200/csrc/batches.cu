@@ -77,17 +77,11 @@ __global__ void __launch_bounds__(kThreads) copy_batches_kernel(const hm_batch *
 
 }  // namespace
 
-size_t batches_work_bytes(const hm_tree *t, int64_t total, int bits) {
-  if (bits <= 0) return 0;
-  return 3 * (size_t)align_up(total * 8, 256) + (size_t)align_up(total * 4, 256) +
-         partition_scratch_bytes(total, bits);
-}
-
-int batch_sort_bits(const hm_tree *t, int64_t total) {
-  if (total > INT32_MAX) return 0;
-  int b = t->cfg.sort_bits;
-  if (b >= 0) return b;
-  return (total >= (1 << 21) && t->n_leaf >= (1 << 16)) ? 16 : 0;
+// Work memory of a large set: the gathered queries, the gathered results and
+// the scratch of the sorted search plan.  Small sets need none.
+size_t batches_work_bytes(const hm_tree *t, int64_t total, const SearchPlan &p) {
+  if (p.bits <= 0) return 0;
+  return 2 * (size_t)align_up(total * 8, 256) + p.scratch;
 }
 
 // Host side: fills the descriptor block image for nb batches.
@@ -116,37 +110,27 @@ int build_set(const hm_tree *t, const hm_batch *batches, int nb, std::vector<cha
 }
 
 // Enqueues the whole multi-batch search on s.  d_set is the device copy of
-// the descriptor block; work has batches_work_bytes(total, bits) bytes.
+// the descriptor block; work has batches_work_bytes(total, plan) bytes.
 int enqueue_batches(hm_tree *t, char *d_set, int nb, int64_t total, int64_t tiles, int64_t copy_tiles,
-                    int bits, char *work, cudaStream_t s) {
+                    const SearchPlan &plan, char *work, cudaStream_t s) {
   const SetLayout l = set_layout(nb);
   const hm_batch *d_b = reinterpret_cast<const hm_batch *>(d_set + l.off_batches);
   const int64_t *qpre = reinterpret_cast<const int64_t *>(d_set + l.off_qpre);
   const int64_t *cpre = reinterpret_cast<const int64_t *>(d_set + l.off_cpre);
   int64_t *tpre = reinterpret_cast<int64_t *>(d_set + l.off_tpre);
   if (total == 0) return HM_OK;
-  if (bits <= 0) {
+  if (plan.bits <= 0) {
     cudaMemsetAsync(tpre + nb + 1, 0, 8, s);
     return launch_search_batches(t, d_b, tpre, nb, tiles, t->cfg.group_width,
                                  t->cfg.queries_per_group, s);
   }
   const size_t a8 = align_up(total * 8, 256);
   int64_t *all_q = reinterpret_cast<int64_t *>(work);
-  int64_t *sorted_q = reinterpret_cast<int64_t *>(work + a8);
-  int64_t *all_out = reinterpret_cast<int64_t *>(work + 2 * a8);
-  int32_t *pos = reinterpret_cast<int32_t *>(work + 3 * a8);
-  void *pscratch = work + 3 * a8 + align_up(total * 4, 256);
+  int64_t *all_out = reinterpret_cast<int64_t *>(work + a8);
   unsigned grid = (unsigned)std::min<int64_t>(copy_tiles, (int64_t)t->num_sms * 8);
   copy_batches_kernel<<<grid, kThreads, 0, s>>>(d_b, qpre, cpre, nb, all_q, 0);
   note_launch();
-  int tok = prof_begin(t, s);
-  int rc = partition_queries(t, all_q, total, bits, sorted_q, pos, pscratch, s);
-  prof_end(t, kStagePartition, tok, s);
-  if (rc) return rc;
-  SearchLaunch sl{sorted_q, all_out, pos, total};
-  tok = prof_begin(t, s);
-  rc = launch_search(t, sl, t->cfg.group_width, t->cfg.queries_per_group, s);
-  prof_end(t, kStageSearch, tok, s);
+  int rc = run_planned_search(t, plan, all_q, total, all_out, s, work + 2 * a8);
   if (rc) return rc;
   copy_batches_kernel<<<grid, kThreads, 0, s>>>(d_b, qpre, cpre, nb, all_out, 1);
   note_launch();
@@ -161,7 +145,7 @@ struct hm_plan {
   hm_tree *tree = nullptr;
   int nb = 0;
   int64_t total = 0, tiles = 0, copy_tiles = 0;
-  int bits = 0;
+  SearchPlan plan;
   char *dev = nullptr;  // descriptor block + work
   size_t dev_bytes = 0;
   std::vector<hm_batch> batches;
@@ -189,9 +173,18 @@ int capture(hm_plan *p) {
   // the tile prefix depends on the search parameters: rebuild and upload it
   int rc0 = build_set(t, p->batches.data(), p->nb, p->img, &p->total, &p->tiles, &p->copy_tiles);
   if (rc0) return rc0;
+  p->plan = plan_search(t, p->total);
+  const size_t need = p->img.size() + batches_work_bytes(t, p->total, p->plan);
+  if (need > p->dev_bytes) {  // a retune may need more work memory
+    if (p->dev) cudaFree(p->dev);
+    p->dev = nullptr;
+    p->dev_bytes = 0;
+    cudaError_t ea = cudaMalloc(&p->dev, need);
+    if (ea != cudaSuccess) return cuda_err(ea);
+    p->dev_bytes = need;
+  }
   cudaError_t e0 = cudaMemcpy(p->dev, p->img.data(), p->img.size(), cudaMemcpyHostToDevice);
   if (e0 != cudaSuccess) return cuda_err(e0);
-  p->bits = batch_sort_bits(t, p->total);
   // warm the kernel attribute / occupancy cache outside the capture
   int rc = launch_search_warm(t, t->cfg.group_width, t->cfg.queries_per_group);
   if (rc) return rc;
@@ -203,7 +196,7 @@ int capture(hm_plan *p) {
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     set_capturing(true);
-    rc = enqueue_batches(t, p->dev, p->nb, p->total, p->tiles, p->copy_tiles, p->bits,
+    rc = enqueue_batches(t, p->dev, p->nb, p->total, p->tiles, p->copy_tiles, p->plan,
                          p->dev + l.bytes, cs);
     set_capturing(false);
     cudaError_t e2 = cudaStreamEndCapture(cs, &p->graph);
@@ -245,15 +238,15 @@ int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream hs)
   int64_t total = 0, tiles = 0, copy_tiles = 0;
   int rc = build_set(t, batches, nb, img, &total, &tiles, &copy_tiles);
   if (rc) return rc;
-  const int bits = batch_sort_bits(t, total);
+  const SearchPlan plan = plan_search(t, total);
   const size_t set_bytes = img.size();
-  rc = ensure_scratch(t, set_bytes + batches_work_bytes(t, total, bits));
+  rc = ensure_scratch(t, set_bytes + batches_work_bytes(t, total, plan));
   if (rc) return rc;
   char *d = static_cast<char *>(t->scratch);
   cudaError_t e = cudaMemcpyAsync(d, img.data(), set_bytes, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return cuda_err(e);
   int tok = prof_begin(t, s);
-  rc = enqueue_batches(t, d, nb, total, tiles, copy_tiles, bits, d + set_bytes, s);
+  rc = enqueue_batches(t, d, nb, total, tiles, copy_tiles, plan, d + set_bytes, s);
   prof_end(t, kStageBatches, tok, s);
   e = cudaStreamSynchronize(s);  // img is a host buffer the copy reads
   if (rc) return rc;
@@ -274,17 +267,9 @@ int hm_plan_create(hm_tree *t, const hm_batch *batches, int nb, hm_plan **out) {
     delete p;
     return rc;
   }
-  // work is sized for the largest pre-sort (16 bits) so a later retune fits
-  p->dev_bytes = p->img.size() + batches_work_bytes(t, p->total, 16);
-  cudaError_t e = cudaMalloc(&p->dev, p->dev_bytes);
-  if (e != cudaSuccess) {
-    if (p->dev) cudaFree(p->dev);
-    delete p;
-    return cuda_err(e);
-  }
-  rc = capture(p);
+  rc = capture(p);  // sizes and allocates the plan's device memory
   if (rc) {
-    cudaFree(p->dev);
+    if (p->dev) cudaFree(p->dev);
     delete p;
     return rc;
   }

@@ -53,7 +53,7 @@ int ensure_scratch(hm_tree *t, size_t bytes) {
 }
 
 static const char *kStageNames[kStageCount] = {"partition", "search", "search_batches", "range",
-                                               "upsert"};
+                                               "upsert", "join", "unpermute"};
 
 static cudaEvent_t prof_event(hm_tree *t) {
   if (!t->prof_pool.empty()) {
@@ -122,6 +122,7 @@ int check_config(const hm_config &c) {
   if (c.sort_bits < -1 || c.sort_bits > 16) return HM_EINVAL;
   if (c.smem_bytes < 0 || c.smem_bytes > 200 * 1024) return HM_EINVAL;
   if (c.cache_hints != 1 && c.cache_hints != 2) return HM_EINVAL;
+  if (c.join != -1 && c.join != 1 && c.join != 2) return HM_EINVAL;
   return HM_OK;
 }
 
@@ -134,6 +135,7 @@ void fill_defaults(hm_config *c) {
   if (c->queries_per_group == 0) c->queries_per_group = 2;
   if (c->smem_bytes == 0) c->smem_bytes = 48 * 1024;
   if (c->cache_hints == 0) c->cache_hints = 1;
+  if (c->join == 0) c->join = -1;
 }
 
 void choose_smem_levels(hm_tree *t) {
@@ -146,16 +148,6 @@ void choose_smem_levels(hm_tree *t) {
     t->smem_levels = l;
     t->smem_nodes = (int)nodes;
   }
-}
-
-// Effective pre-sort bits for a batch of n queries (0 = no pre-sort).
-int sort_bits_for(const hm_tree *t, int64_t n) {
-  if (n > INT32_MAX) return 0;  // positions are carried as int32
-  int b = t->cfg.sort_bits;
-  if (b >= 0) return b;
-  // auto: pre-sort large batches on 16 bits (two stable passes); small
-  // batches cannot amortise the passes.
-  return (n >= (1 << 21) && t->n_leaf >= (1 << 16)) ? 16 : 0;
 }
 
 cudaStream_t as_stream(hm_stream s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -204,46 +196,75 @@ int ensure_pinned(hm_tree *t, size_t bytes) {
   return HM_OK;
 }
 
-// Search of device-resident queries on stream s, with the optional pre-sort.
+// Search of device-resident queries on stream s by the plan for n queries.
 int search_device(hm_tree *t, const int64_t *d_q, int64_t n, int64_t *d_out, cudaStream_t s,
                   void *scratch_base, size_t scratch_avail) {
-  int bits = sort_bits_for(t, n);
-  if (bits > 0) {
-    size_t need = (size_t)align_up(n * 8, 256) + (size_t)align_up(n * 4, 256) +
-                  partition_scratch_bytes(n, bits);
-    if (need <= scratch_avail) {
-      char *p = static_cast<char *>(scratch_base);
-      int64_t *qs = reinterpret_cast<int64_t *>(p);
-      int32_t *pos = reinterpret_cast<int32_t *>(p + align_up(n * 8, 256));
-      void *ps = p + align_up(n * 8, 256) + align_up(n * 4, 256);
-      int tok = prof_begin(t, s);
-      int rc = partition_queries(t, d_q, n, bits, qs, pos, ps, s);
-      prof_end(t, kStagePartition, tok, s);
-      if (rc) return rc;
-      SearchLaunch l{qs, d_out, pos, n};
-      tok = prof_begin(t, s);
-      rc = launch_search(t, l, t->cfg.group_width, t->cfg.queries_per_group, s);
-      prof_end(t, kStageSearch, tok, s);
-      return rc;
-    }
-  }
-  SearchLaunch l{d_q, d_out, nullptr, n};
-  int tok = prof_begin(t, s);
-  int rc = launch_search(t, l, t->cfg.group_width, t->cfg.queries_per_group, s);
-  prof_end(t, kStageSearch, tok, s);
-  return rc;
+  const SearchPlan p = plan_search(t, n);
+  if (p.scratch > scratch_avail) return HM_ENOMEM;
+  return run_planned_search(t, p, d_q, n, d_out, s, scratch_base);
 }
 
-size_t search_scratch_need(const hm_tree *t, int64_t n) {
-  int bits = sort_bits_for(t, n);
-  if (bits <= 0) return 0;
-  return (size_t)align_up(n * 8, 256) + (size_t)align_up(n * 4, 256) +
-         partition_scratch_bytes(n, bits);
-}
+size_t search_scratch_need(const hm_tree *t, int64_t n) { return plan_search(t, n).scratch; }
 
 }  // namespace
 
 namespace hm {
+
+SearchPlan plan_search(const hm_tree *t, int64_t n) {
+  SearchPlan p;
+  if (n <= 0 || n > INT32_MAX) return p;  // positions are carried as int32
+  const hm_config &c = t->cfg;
+  const bool join = (c.join == 1 && (c.leaf_cap == 16 || c.leaf_cap == 64)) ||
+                    (c.join == -1 && n >= std::max<int64_t>((int64_t)1 << 22, 4 * (int64_t)t->n_leaf) &&
+                     t->n_leaf >= 1024 && join_fits(t));  // measured: wins from ~4 queries per leaf
+  if (join) {
+    p.join = true;
+    p.bits = join_bits(t);
+  } else {
+    p.bits = c.sort_bits > 0 ? c.sort_bits : 0;
+  }
+  if (p.bits > 0) {  // grouped queries, grouped results, partition (offset mode), join
+    p.scratch = 2 * (size_t)align_up(n * 8, 256) + partition_scratch_bytes(n, p.bits, true);
+    if (p.join) p.scratch += join_scratch_bytes(n, p.bits);
+  }
+  return p;
+}
+
+int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int64_t n, int64_t *d_out,
+                       cudaStream_t s, void *scratch) {
+  if (n <= 0) return HM_OK;
+  if (p.bits <= 0) {
+    SearchLaunch l{d_q, d_out, nullptr, n};
+    int tok = prof_begin(t, s);
+    int rc = launch_search(t, l, t->cfg.group_width, t->cfg.queries_per_group, s);
+    prof_end(t, kStageSearch, tok, s);
+    return rc;
+  }
+  char *b = static_cast<char *>(scratch);
+  int64_t *qs = reinterpret_cast<int64_t *>(b);
+  int64_t *res = reinterpret_cast<int64_t *>(b + align_up(n * 8, 256));
+  char *ps = b + 2 * align_up(n * 8, 256);
+  const int64_t *bstart = nullptr;
+  int tok = prof_begin(t, s);
+  int rc = partition_queries(t, d_q, n, p.bits, qs, nullptr, ps, s, &bstart);
+  prof_end(t, kStagePartition, tok, s);
+  if (rc) return rc;
+  tok = prof_begin(t, s);
+  if (p.join) {
+    rc = launch_join(t, qs, bstart, p.bits, n, res, ps + partition_scratch_bytes(n, p.bits, true), s);
+    prof_end(t, kStageJoin, tok, s);
+  } else {
+    SearchLaunch l{qs, res, nullptr, n};
+    rc = launch_search(t, l, t->cfg.group_width, t->cfg.queries_per_group, s);
+    prof_end(t, kStageSearch, tok, s);
+  }
+  if (rc) return rc;
+  tok = prof_begin(t, s);
+  rc = unpermute_results(n, p.bits, res, d_out, ps, s);
+  prof_end(t, kStageUnpermute, tok, s);
+  return rc;
+}
+
 // Entry points into this file's helpers for the other host sources.
 int run_search(hm_tree *t, const int64_t *d_q, int64_t n, int64_t *d_out, cudaStream_t s,
                void *scratch, size_t scratch_bytes) {
@@ -451,6 +472,7 @@ int hm_set_search_config(hm_tree *t, const hm_config *cfg) {
   c.sort_bits = cfg->sort_bits;
   if (cfg->smem_bytes) c.smem_bytes = cfg->smem_bytes;
   if (cfg->cache_hints) c.cache_hints = cfg->cache_hints;
+  if (cfg->join) c.join = cfg->join;
   int rc = check_config(c);
   if (rc) return rc;
   t->cfg = c;
@@ -715,36 +737,46 @@ int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n_, hm_config *best)
   const int qpgs[] = {1, 2, 4};
   const int bits_list[] = {0, 8, 12, 16};
   const int hints_list[] = {1, 2};
-  int rc = HM_OK;
+  std::vector<hm_config> cands;
   for (int w : widths)
     for (int q : qpgs)
       for (int bits : bits_list)
         for (int hints : hints_list) {
-        hm_config c = orig;
-        c.group_width = w;
-        c.queries_per_group = q;
-        c.sort_bits = bits;
-        c.cache_hints = hints;
-        t->cfg = c;
-        choose_smem_levels(t);
-        rc = ensure_scratch(t, search_scratch_need(t, n));
-        if (rc) break;
-        float ms = 1e30f;
-        for (int rep = 0; rep < 3 && rc == HM_OK; rep++) {
-          cudaEventRecord(a, 0);
-          rc = search_device(t, sample_q, n, d_out, 0, t->scratch, t->scratch_bytes);
-          cudaEventRecord(b, 0);
-          cudaEventSynchronize(b);
-          float x = 0;
-          cudaEventElapsedTime(&x, a, b);
-          if (rep > 0 && x < ms) ms = x;
+          hm_config c = orig;
+          c.group_width = w;
+          c.queries_per_group = q;
+          c.sort_bits = bits;
+          c.cache_hints = hints;
+          c.join = 2;
+          cands.push_back(c);
         }
-        if (rc) break;
-        if (ms < best_ms) {
-          best_ms = ms;
-          best_cfg = c;
-        }
-      }
+  {
+    hm_config c = orig;  // the bucket join (its own bucket bits)
+    c.join = 1;
+    cands.push_back(c);
+  }
+  int rc = HM_OK;
+  for (const hm_config &c : cands) {
+    t->cfg = c;
+    choose_smem_levels(t);
+    rc = ensure_scratch(t, search_scratch_need(t, n));
+    if (rc) break;
+    float ms = 1e30f;
+    for (int rep = 0; rep < 3 && rc == HM_OK; rep++) {
+      cudaEventRecord(a, 0);
+      rc = search_device(t, sample_q, n, d_out, 0, t->scratch, t->scratch_bytes);
+      cudaEventRecord(b, 0);
+      cudaEventSynchronize(b);
+      float x = 0;
+      cudaEventElapsedTime(&x, a, b);
+      if (rep > 0 && x < ms) ms = x;
+    }
+    if (rc) break;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best_cfg = c;
+    }
+  }
   t->cfg = rc ? orig : best_cfg;
   choose_smem_levels(t);
   cudaEventDestroy(a);

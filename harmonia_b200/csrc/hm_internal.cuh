@@ -57,6 +57,35 @@ struct DevTree {
   int32_t cache_hints; // 1: L2 evict_last for inner rows, evict_first for leaves
 };
 
+#ifdef __CUDACC__
+// One thread's descent to the leaf whose key range holds q: at each inner row
+// count the index words <= q (index word w mirrors key slot 8(w+1)) to pick an
+// 8-key slice, then the slice's keys <= q; child = first child + count
+// (open-harmonia/src/avx.cpp:2-54 counts separators <= key the same way).
+// Inner rows are read-only while any caller runs.
+__device__ __forceinline__ int32_t descend_leaf(const DevTree &t, int f, int64_t q) {
+  const int ix = f / 8, row = ix + f;
+  int32_t node = 0;
+  for (int l = 0; l < t.height; l++) {
+    const int64_t *r = t.inner + (int64_t)node * row;
+    int k = 0;
+    for (int v = 0; v < ix / 2; v++) {
+      const longlong2 p = __ldg(reinterpret_cast<const longlong2 *>(r + 2 * v));
+      k += (p.x <= q) + (p.y <= q);
+    }
+    k = min(k, ix - 1);
+    int c = 8 * k;
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const longlong2 p = __ldg(reinterpret_cast<const longlong2 *>(r + ix + 8 * k + 2 * v));
+      c += (p.x <= q) + (p.y <= q);
+    }
+    node = __ldg(t.prefix + node) + c;
+  }
+  return node - t.n_inner;
+}
+#endif
+
 __host__ __device__ inline int64_t part_start(int64_t j, int64_t total, int64_t parts) {
   int64_t q = total / parts, r = total % parts;
   return j * q + (j < r ? j : r);
@@ -168,9 +197,19 @@ int launch_search_warm(const hm_tree *t, int group_width, int qpg);
 size_t search_smem_bytes(const hm_tree *t);
 
 // ---- query pre-sort (partition.cu) ----
-size_t partition_scratch_bytes(int64_t n, int bits);
+// offsets: the partition keeps chunk offsets in the scratch for
+// unpermute_results (pos_out == nullptr); else it writes input positions.
+size_t partition_scratch_bytes(int64_t n, int bits, bool offsets);
+// Groups queries by the top `bits` bits of their key (relative to the tree's
+// key range); *bucket_start (if given) receives a device pointer, inside the
+// scratch, to the 2^bits + 1 bucket starts.  pos_out: original position of
+// each grouped query, or nullptr for the offset mode.
 int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits,
-                      int64_t *q_out, int32_t *pos_out, void *scratch, cudaStream_t s);
+                      int64_t *q_out, int32_t *pos_out, void *scratch, cudaStream_t s,
+                      const int64_t **bucket_start = nullptr);
+// Offset mode: out[i] = result of input query i, given the results in grouped
+// order (res_sorted, clobbered) and the scratch of the matching partition.
+int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, void *scratch, cudaStream_t s);
 
 // ---- scan, export, range (misc.cu) ----
 void scan_counts(int64_t *counts, int64_t m, cudaStream_t s);  // one-CTA in-place exclusive scan
@@ -190,10 +229,31 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
                  int flags, cudaStream_t s);
 
 // ---- stage timing ----
-enum Stage { kStagePartition = 0, kStageSearch, kStageBatches, kStageRange, kStageUpsert, kStageCount };
+enum Stage { kStagePartition = 0, kStageSearch, kStageBatches, kStageRange, kStageUpsert, kStageJoin,
+             kStageUnpermute, kStageCount };
 // Records the start event of a stage on stream s (no-op unless profiling).
 int prof_begin(hm_tree *t, cudaStream_t s);
 void prof_end(hm_tree *t, int stage, int token, cudaStream_t s);
+
+// ---- bucket join (join.cu) ----
+int join_bits(const hm_tree *t);   // bucket bits for the join (leaves per bucket fit shared memory)
+bool join_fits(const hm_tree *t);  // the join supports this leaf size and its buckets fit on average
+size_t join_scratch_bytes(int64_t n, int bits);
+int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int bits,
+                int64_t n, int64_t *out, void *scratch, cudaStream_t s);
+
+// ---- search plan (harmonia.cu) ----
+// How a batch of n queries is searched: NTG descent on the batch as given
+// (bits = 0), after a pre-sort (bits > 0, join = false), or pre-sort +
+// bucket join; scratch = bytes of working memory it needs.
+struct SearchPlan {
+  int bits = 0;
+  bool join = false;
+  size_t scratch = 0;
+};
+SearchPlan plan_search(const hm_tree *t, int64_t n);
+int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int64_t n, int64_t *d_out,
+                       cudaStream_t s, void *scratch);
 
 // ---- host helpers (harmonia.cu) ----
 // Point search of device-resident queries on s, with the configured pre-sort;

@@ -1,0 +1,313 @@
+// Bucket join: point search for a pre-sorted batch that is large relative to
+// the tree.
+//
+// After the query pre-sort (partition.cu) the queries of one bucket form a
+// contiguous run and the bucket's keys lie in a contiguous range of leaves.
+// Instead of one descent per query (search.cu), a CTA takes a run of one
+// bucket, copies the bucket's leaf records (keys and values, 256 B per
+// 16-key leaf) from HBM into shared memory with 16-B loads in order, and
+// answers every query of the run from shared memory: a binary search over the
+// leaves' first keys picks the leaf, a scan of its keys the slot.  The leaf
+// range of each bucket comes from one descent per bucket boundary (a
+// separate kernel, one thread per boundary).  Leaves are read once per run
+// and sequentially, so the DRAM traffic of a batch with more queries than
+// leaves falls from a random 160 B per query to the size of the touched leaf
+// region.  A bucket whose leaves do not fit shared memory (very skewed keys)
+// falls back to a scalar descent per query.
+//
+// The per-query semantics are the reference's (child = number of separators
+// <= key, open-harmonia/src/avx.cpp:2-54; equality in the leaf,
+// open-harmonia/src/bpt.h:252-274): a key routed to leaf j lies between
+// leaf j's first key and leaf j+1's first key, so the largest leaf of the
+// range whose first key is <= q is the leaf the descent would reach.
+#include "hm_internal.cuh"
+
+#include <algorithm>
+
+namespace hm {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPerThread = 4;
+constexpr int kRun = kThreads * kPerThread;  // queries per work item
+constexpr int kStageMax = 96 * 1024;         // shared memory of one stage, at most
+
+// A work item: a run of at most kRun queries of one bucket and the bucket's
+// leaves [l0, l0 + nl).
+struct __align__(16) Item {
+  int32_t qa, len, l0, nl;
+};
+
+// Per bucket b in [0, nb]: leafb[b] = leaf holding the smallest key of bucket
+// b (bucket b's keys lie in leaves [leafb[b], leafb[b+1]]) and cnt[b] = its
+// work items (0 for b = nb).
+__global__ void bucket_prep_kernel(DevTree t, int f, int64_t lo, int shift, int nb,
+                                   const int64_t *__restrict__ bstart, int32_t *__restrict__ leafb,
+                                   int32_t *__restrict__ cnt) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x) {
+    cnt[b] = b < nb ? (int32_t)((bstart[b + 1] - bstart[b] + kRun - 1) / kRun) : 0;
+    if (b == 0) {
+      leafb[0] = 0;
+      continue;
+    }
+    if (b == nb) {
+      leafb[nb] = t.n_leaf - 1;
+      continue;
+    }
+    const uint64_t off = (uint64_t)b << shift;
+    if (off >= (uint64_t)kMaxKey - (uint64_t)lo) {  // boundary at or past Max_Key: no key above it
+      leafb[b] = t.n_leaf - 1;
+      continue;
+    }
+    leafb[b] = descend_leaf(t, f, (int64_t)((uint64_t)lo + off));
+  }
+}
+
+// Bucket b's items start at first[b] (exclusive scan of cnt).
+__global__ void expand_items_kernel(int nb, const int64_t *__restrict__ bstart, const int32_t *__restrict__ leafb,
+                                    const int32_t *__restrict__ cnt, const int64_t *__restrict__ first,
+                                    Item *__restrict__ items) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const int c = cnt[b];
+    if (c == 0) continue;
+    const int64_t s = bstart[b], e = bstart[b + 1];
+    const int32_t l0 = leafb[b], nl = leafb[b + 1] - l0 + 1;
+    int64_t o = first[b];
+    for (int r = 0; r < c; r++) {
+      Item it;
+      it.qa = (int32_t)(s + (int64_t)r * kRun);
+      it.len = (int32_t)min((int64_t)kRun, e - (s + (int64_t)r * kRun));
+      it.l0 = l0;
+      it.nl = nl;
+      items[o + r] = it;
+    }
+  }
+}
+
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Words of one leaf in a stage: its keys at a stride of LC + 1 (leaf m's key s
+// at m * (LC + 1) + s, so lanes reading different leaves fall in different
+// banks), then, after all keys, its values densely (m * LC + s).
+template <int LC>
+__host__ __device__ constexpr int stage_leaf_bytes() {
+  return (2 * LC + 1) * 8;
+}
+
+template <int LC>
+struct Stage {
+  int64_t *kp, *vp;
+  __device__ Stage(int64_t *base, int ml) : kp(base), vp(base + ml * (LC + 1)) {}
+};
+
+// Asynchronous copy of an item's leaf records into a stage (nothing when the
+// leaves do not fit; such an item takes the scalar path).
+template <int LC>
+__device__ __forceinline__ void stage_leaves(const DevTree &t, const Item &it, Stage<LC> st, int ml) {
+  constexpr int LI = LC >= 32 ? LC / 8 : 0;
+  constexpr int ROW = LI + 2 * LC;
+  constexpr int KS = LC + 1;
+  if (it.nl < 1 || it.nl > ml) return;
+  const longlong2 *src = reinterpret_cast<const longlong2 *>(t.leaf_rows + (int64_t)it.l0 * ROW);
+  const int nvec = it.nl * (ROW / 2);
+  for (int v = threadIdx.x; v < nvec; v += kThreads) {
+    const int m = v / (ROW / 2), w = 2 * (v - m * (ROW / 2));
+    if (w < LI) continue;
+    if (w < LI + LC) {
+      cp_async8(st.kp + m * KS + (w - LI), reinterpret_cast<const int64_t *>(src + v));
+      cp_async8(st.kp + m * KS + (w - LI) + 1, reinterpret_cast<const int64_t *>(src + v) + 1);
+    } else {
+      cp_async16(st.vp + m * LC + (w - LI - LC), src + v);
+    }
+  }
+}
+
+template <int LC>
+__device__ __forceinline__ int64_t lookup_staged(Stage<LC> st, int nl, int span, int64_t q) {
+  constexpr int KS = LC + 1;
+  // leaf: the last of [1, nl) whose first key is <= q, else 0
+  int m = 0;
+  for (int step = span >> 1; step > 0; step >>= 1)
+    if (m + step < nl && st.kp[(m + step) * KS] <= q) m += step;
+  // slot: the last key <= q among the leaf's sorted keys (Max_Key pads the
+  // tail), else slot 0
+  const int64_t *kr = st.kp + m * KS;
+  int c = 0;
+#pragma unroll
+  for (int step = LC / 2; step > 0; step >>= 1)
+    if (kr[c + step] <= q) c += step;
+  return kr[c] == q ? st.vp[m * LC + c] : HM_NOT_FOUND;
+}
+
+template <int LC>
+__device__ __noinline__ int64_t lookup_scalar(const DevTree &t, int f, int64_t q) {
+  constexpr int LI = LC >= 32 ? LC / 8 : 0;
+  constexpr int ROW = LI + 2 * LC;
+  const int32_t leaf = descend_leaf(t, f, q);
+  const int64_t *kr = t.leaf_rows + (int64_t)leaf * ROW + LI;
+  int64_t v = HM_NOT_FOUND;
+#pragma unroll 4
+  for (int s = 0; s < LC; s++)
+    if (__ldg(kr + s) == q) v = __ldg(kr + LC + s);
+  return v;
+}
+
+// Persistent CTAs walk the items with a stride of the grid; two stages: the
+// leaves of the next item are copied (cp.async) while the current one is
+// answered from shared memory.  Item descriptors and the queries of the next
+// item are loaded one iteration ahead.  Results are written in the grouped
+// order (out[i] for grouped query i).
+template <int LC>
+__global__ void __launch_bounds__(kThreads, 4) join_kernel(DevTree t, int f, const Item *__restrict__ items,
+                                                        const int64_t *__restrict__ nitems,
+                                                        const int64_t *__restrict__ qs, int64_t *__restrict__ out,
+                                                        int ml) {
+  extern __shared__ __align__(16) int64_t smem[];
+  const int stage_words = ml * (2 * LC + 1);
+  const int64_t n_items = *nitems;
+  const int64_t g = gridDim.x;
+  int64_t it = blockIdx.x;
+  if (it >= n_items) return;
+  const Item none{0, 0, 0, 0};
+  Item cur = items[it];
+  Item nxt = it + g < n_items ? items[it + g] : none;
+  stage_leaves<LC>(t, cur, Stage<LC>(smem, ml), ml);
+  cp_async_commit();
+  int64_t q[kPerThread];
+#pragma unroll
+  for (int j = 0; j < kPerThread; j++) {
+    const int r = j * kThreads + threadIdx.x;
+    q[j] = r < cur.len ? __ldg(qs + cur.qa + r) : 0;
+  }
+  for (int k = 0; it < n_items; k++, it += g) {
+    Stage<LC> st(smem + (k & 1) * stage_words, ml);
+    // next item: its leaves into the other stage, its descriptor after it
+    stage_leaves<LC>(t, nxt, Stage<LC>(smem + ((k + 1) & 1) * stage_words, ml), ml);
+    cp_async_commit();
+    const Item after = it + 2 * g < n_items ? items[it + 2 * g] : none;
+    int64_t qn[kPerThread];
+#pragma unroll
+    for (int j = 0; j < kPerThread; j++) {
+      const int r = j * kThreads + threadIdx.x;
+      qn[j] = r < nxt.len ? __ldg(qs + nxt.qa + r) : 0;
+    }
+    cp_async_wait_prev();
+    __syncthreads();
+    const bool staged = cur.nl >= 1 && cur.nl <= ml;
+    int span = 1;
+    while (span < cur.nl) span <<= 1;
+#pragma unroll
+    for (int j = 0; j < kPerThread; j++) {
+      const int r = j * kThreads + threadIdx.x;
+      if (r >= cur.len) continue;
+      int64_t v = HM_NOT_FOUND;
+      if (q[j] != kMaxKey) v = staged ? lookup_staged<LC>(st, cur.nl, span, q[j]) : lookup_scalar<LC>(t, f, q[j]);
+      out[cur.qa + r] = v;  // grouped order: consecutive threads, consecutive slots
+    }
+    __syncthreads();  // the stage is refilled two items later
+    cur = nxt;
+    nxt = after;
+#pragma unroll
+    for (int j = 0; j < kPerThread; j++) q[j] = qn[j];
+  }
+  cp_async_wait_all();
+}
+
+int64_t max_items(int64_t n, int nb) { return n / kRun + nb + 1; }
+
+int leaf_bytes(int lc) { return lc == 16 ? stage_leaf_bytes<16>() : stage_leaf_bytes<64>(); }
+
+// Leaves one stage holds: room for 1.5x the mean leaves per bucket plus a
+// margin, as an even count (keeps the value part 16-B aligned).
+int stage_leaves_for(const hm_tree *t, int bits) {
+  const int64_t mean = (t->n_leaf + ((int64_t)1 << bits) - 1) >> bits;
+  int64_t ml = mean + mean / 2 + 8;
+  ml = std::min<int64_t>(ml, kStageMax / leaf_bytes(t->cfg.leaf_cap));
+  return (int)(ml & ~int64_t(1));
+}
+
+}  // namespace
+
+int join_bits(const hm_tree *t) {
+  // 16 bits, or fewer while buckets still average at most 32 leaves
+  int b = 1;
+  while (b < 16 && (t->n_leaf >> b) > 32) b++;
+  return b;
+}
+
+bool join_fits(const hm_tree *t) {
+  if (t->cfg.leaf_cap != 16 && t->cfg.leaf_cap != 64) return false;
+  const int bits = join_bits(t);
+  const int64_t mean = (t->n_leaf + ((int64_t)1 << bits) - 1) >> bits;
+  return mean + mean / 2 + 8 <= stage_leaves_for(t, bits) + 1;
+}
+
+size_t join_scratch_bytes(int64_t n, int bits) {
+  const int64_t nb = (int64_t)1 << bits;
+  return (size_t)(2 * align_up(4 * (nb + 1), 256) + align_up(8 * (nb + 2), 256) +
+                  align_up((int64_t)scan_scratch_bytes(nb + 1), 256) +
+                  align_up((int64_t)sizeof(Item) * max_items(n, (int)nb), 256)) +
+         256;
+}
+
+int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int bits,
+                int64_t n, int64_t *out, void *scratch, cudaStream_t s) {
+  if (n <= 0) return HM_OK;
+  const int nb = 1 << bits;
+  char *p = static_cast<char *>(scratch);
+  int32_t *leafb = reinterpret_cast<int32_t *>(p);
+  p += align_up(4 * (nb + 1), 256);
+  int32_t *cnt = reinterpret_cast<int32_t *>(p);
+  p += align_up(4 * (nb + 1), 256);
+  int64_t *first = reinterpret_cast<int64_t *>(p);
+  p += align_up(8 * (nb + 2), 256);
+  void *scan = p;
+  p += align_up((int64_t)scan_scratch_bytes(nb + 1), 256);  // keeps the 16-B items aligned
+  Item *items = reinterpret_cast<Item *>(p);
+  // bucket geometry, as the partition computed it
+  uint64_t range = (uint64_t)t->key_max - (uint64_t)t->key_min;
+  int len = 0;
+  while (len < 64 && (range >> len) != 0) len++;
+  const int shift = len > bits ? len - bits : 0;
+  const unsigned gb = (unsigned)((nb + 1 + 255) / 256);
+  bucket_prep_kernel<<<gb, 256, 0, s>>>(t->view(), t->cfg.fanout, t->key_min, shift, nb, bstart, leafb, cnt);
+  exclusive_scan_i32(cnt, first, nb + 1, scan, s);
+  expand_items_kernel<<<gb, 256, 0, s>>>(nb, bstart, leafb, cnt, first, items);
+  const int lc = t->cfg.leaf_cap;
+  const int ml = stage_leaves_for(t, bits);
+  const size_t smem = (size_t)2 * ml * leaf_bytes(lc);
+  const int per_sm = std::max(1, std::min(8, (int)((227 * 1024) / (smem + 1024))));
+  const unsigned grid = (unsigned)std::min<int64_t>(max_items(n, nb), (int64_t)t->num_sms * per_sm);
+  static bool attr_set = false;  // opt in to > 48 KiB of shared memory once
+  if (!attr_set) {
+    cudaFuncSetAttribute(join_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kStageMax);
+    cudaFuncSetAttribute(join_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kStageMax);
+    cudaFuncSetAttribute(join_kernel<16>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(join_kernel<64>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    attr_set = true;
+  }
+  if (lc == 16) {
+    join_kernel<16><<<grid, kThreads, smem, s>>>(t->view(), t->cfg.fanout, items, first + nb, qs, out, ml);
+  } else if (lc == 64) {
+    join_kernel<64><<<grid, kThreads, smem, s>>>(t->view(), t->cfg.fanout, items, first + nb, qs, out, ml);
+  } else {
+    return HM_EINVAL;
+  }
+  note_launch(3);
+  return cuda_err(cudaGetLastError());
+}
+
+}  // namespace hm

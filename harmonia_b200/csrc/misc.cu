@@ -89,28 +89,6 @@ __global__ void export_kernel(DevTree t, int lc, int li, int64_t *__restrict__ k
   }
 }
 
-// Scalar descent to the leaf holding the position of q (one thread).
-__device__ __forceinline__ int32_t descend_scalar(const DevTree &t, int f, int64_t q) {
-  const int ix = f / 8, row = ix + f;
-  int32_t node = 0;
-  for (int l = 0; l < t.height; l++) {
-    const int64_t *r = t.inner + (int64_t)node * row;
-    int k = 0;
-    for (int v = 0; v < ix / 2; v++) {
-      longlong2 p = __ldg(reinterpret_cast<const longlong2 *>(r + 2 * v));
-      k += (p.x <= q) + (p.y <= q);
-    }
-    k = min(k, ix - 1);
-    int c = 8 * k;
-    for (int v = 0; v < 4; v++) {
-      longlong2 p = __ldg(reinterpret_cast<const longlong2 *>(r + ix + 8 * k + 2 * v));
-      c += (p.x <= q) + (p.y <= q);
-    }
-    node = __ldg(t.prefix + node) + c;
-  }
-  return node - t.n_inner;
-}
-
 __global__ void range_locate_kernel(DevTree t, int f, int lc, int li, const int64_t *__restrict__ start,
                                     const int32_t *__restrict__ len, int64_t n,
                                     int32_t *__restrict__ first_leaf, int32_t *__restrict__ first_slot,
@@ -125,7 +103,7 @@ __global__ void range_locate_kernel(DevTree t, int f, int lc, int li, const int6
       count[i] = 0;
       continue;
     }
-    int32_t leaf = descend_scalar(t, f, s);
+    int32_t leaf = descend_leaf(t, f, s);
     const int64_t *kr = t.leaf_rows + (int64_t)leaf * (li + 2 * lc) + li;
     int cnt = __ldg(t.leaf_cnt + leaf);
     int lb = 0;  // first slot with key >= start

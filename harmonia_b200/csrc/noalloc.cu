@@ -83,7 +83,7 @@ extern "C" int hm_search_noalloc(hm_tree *t, const int64_t *q, size_t n_, int64_
   if (n > kMaxQueries) return HM_ETOOLARGE;
   if (!device_accessible(q) || !device_accessible(out)) return HM_EINVAL;
   static_assert(kQBytes + kPosBytes + 3 * 256 <= kScratchBytes, "scratch layout");
-  if (partition_scratch_bytes(kMaxQueries, kBits) + kQBytes + kPosBytes + 3 * 256 > kScratchBytes)
+  if (partition_scratch_bytes(kMaxQueries, kBits, false) + kQBytes + kPosBytes + 3 * 256 > kScratchBytes)
     return HM_ETOOLARGE;
   void *base = nullptr;
   int rc = scratch_address(&base);

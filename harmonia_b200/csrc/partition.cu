@@ -1,17 +1,32 @@
 // Query pre-sort (the reference's PSA, "partially sorted aggregation"):
-// order a batch of queries by the top `bits` bits of their key, relative to
-// the tree's key range, and carry each query's original position along.
+// group a batch of queries by the top `bits` bits of their key, relative to
+// the tree's key range, report where each bucket starts, and afterwards move
+// per-query results from the grouped order back to the caller's order.
 //
 // The reference runs cub::DeviceRadixSort::SortPairs on bits [48,64) of
 // (key, pos) before every search launch
 // (open-harmonia/src/full-multi-prefix-sort-8thread.cu:305-309,
 // open-harmonia/regular_bpt/prefix-sort.cu:288-293) and scatters results back
-// through the permutation on the host.  Here the digit is taken relative to
-// [key_min, key_max] of the tree so that all 2^bits buckets cover loaded keys
-// (fixed bits [48,64) leave half of them empty for non-negative keys); up to
-// 8 bits take one stable counting-sort pass, up to 16 bits two (LSD: low
-// part first).  The search then writes each result to out[pos].
-#include "radix_pass.cuh"
+// through the permutation on the host.  Here:
+//   * the bucket is taken relative to [key_min, key_max] of the tree so every
+//     bucket holds loaded keys (fixed bits [48,64) leave half of them empty for
+//     non-negative keys);
+//   * order inside a bucket does not matter, so the passes are unstable and
+//     take their slots with shared-memory atomics;
+//   * up to 8 bits take one pass; more take two, most significant first: the
+//     second pass partitions every first-pass bucket on its own, in chunks that
+//     never straddle a bucket, with offsets from one global scan of counts laid
+//     out as [bucket][digit][chunk];
+//   * each pass stages a 4096-query tile in shared memory grouped by digit and
+//     writes it out so consecutive threads store consecutive slots;
+//   * the payload is either the query's input position (int32, for callers
+//     that scatter results themselves) or its offset inside its 8192-query
+//     input chunk (uint16).  With offsets, unpermute_results undoes the passes
+//     in reverse: per input chunk one CTA reads the chunk's digit runs (each
+//     contiguous), places every result at its offset in shared memory and
+//     writes the chunk out in order, so no pass writes single 8-byte values
+//     at random addresses.
+#include "hm_internal.cuh"
 
 #include <algorithm>
 
@@ -19,27 +34,309 @@ namespace hm {
 
 namespace {
 
-// Bits [sub_shift, sub_shift + 8) of the clamped bucket of a key.
-struct KeyDigit {
+constexpr int kThreads = 256;
+constexpr int kTile = 4096;
+constexpr int kPer = kTile / kThreads;
+constexpr int64_t kChunk = 8192;  // queries per CTA chunk (a multiple of kTile; offsets fit 16 bits)
+constexpr int kRevThreads = 512;
+
+// Bucket of a key: top `bits` bits of (k - lo) over the tree's key range.
+struct Bucket {
   int64_t lo, hi;
   int shift;
   int maxd;
-  int sub_shift;
-  int sub_mask;
   __device__ __forceinline__ int operator()(int64_t k) const {
-    int full;
-    if (k <= lo)
-      full = 0;
-    else if (k >= hi)
-      full = maxd;
-    else
-      full = (int)((uint64_t)(k - lo) >> shift);
-    return (full >> sub_shift) & sub_mask;
+    if (k <= lo) return 0;
+    if (k >= hi) return maxd;
+    return (int)(((uint64_t)k - (uint64_t)lo) >> shift);
   }
 };
 
-KeyDigit make_digit(const hm_tree *t, int bits) {
-  KeyDigit d;
+// A chunk: a contiguous input range inside one first-pass bucket.
+struct Chunk {
+  int64_t begin, end;
+  int32_t bucket;   // first-pass bucket (0 in the first pass)
+  int32_t idx;      // chunk index inside its bucket
+  int32_t nchunks;  // chunks of its bucket
+  int32_t base;     // global index of the bucket's first chunk
+};
+
+// Counts of a pass are laid out [bucket][digit][chunk in bucket]: chunk c of
+// bucket b, digit d at base_b * 256 + d * nchunks_b + c.  One global exclusive
+// scan turns them into output offsets grouped by bucket, then digit.
+__device__ __forceinline__ int64_t count_index(const Chunk &c, int d) {
+  return (int64_t)c.base * 256 + (int64_t)d * c.nchunks + c.idx;
+}
+
+__global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__restrict__ q, const Chunk *__restrict__ chunks,
+                                                        const int32_t *__restrict__ nchunks_total, Bucket bk,
+                                                        int shift2, int mask2, int64_t *__restrict__ counts) {
+  __shared__ unsigned hist[256];
+  if ((int)blockIdx.x >= *nchunks_total) return;
+  const Chunk c = chunks[blockIdx.x];
+  for (int i = threadIdx.x; i < 256; i += kThreads) hist[i] = 0;
+  __syncthreads();
+  for (int64_t base = c.begin; base < c.end; base += 8 * kThreads) {
+    int64_t k[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {  // all loads first
+      const int64_t i = base + j * kThreads + threadIdx.x;
+      k[j] = i < c.end ? __ldg(q + i) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      if (base + j * kThreads + threadIdx.x < c.end) atomicAdd(&hist[(bk(k[j]) >> shift2) & mask2], 1u);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d <= mask2; d += kThreads) counts[count_index(c, d)] = hist[d];
+}
+
+// Payload of the element at input position i of chunk c: loaded from pay_in
+// (LOAD), else generated: the position i (int32) or its offset i - c.begin
+// inside the chunk (uint16).
+template <typename T, bool LOAD>
+__device__ __forceinline__ T payload_of(const T *__restrict__ pay_in, const Chunk &c, int64_t i) {
+  if constexpr (LOAD) {
+    return __ldg(pay_in + i);
+  } else if constexpr (sizeof(T) == 2) {
+    return (T)(i - c.begin);
+  } else {
+    return (T)i;
+  }
+}
+
+template <typename T>
+constexpr int stage_bytes() {
+  return kTile * (8 + (int)sizeof(T) + 1);  // staged keys, payloads, digits
+}
+
+template <typename T, bool LOAD>
+__global__ void __launch_bounds__(kThreads, 3) psa_scatter_kernel(const int64_t *__restrict__ q, const T *__restrict__ pay_in,
+                                                           const Chunk *__restrict__ chunks,
+                                                           const int32_t *__restrict__ nchunks_total, Bucket bk,
+                                                           int shift2, int mask2, const int64_t *__restrict__ offs,
+                                                           int64_t *__restrict__ q_out, T *__restrict__ pay_out) {
+  extern __shared__ __align__(16) unsigned char stage[];  // stage_bytes<T>(), dynamic
+  int64_t *sk = reinterpret_cast<int64_t *>(stage);
+  T *sp = reinterpret_cast<T *>(stage + kTile * 8);
+  unsigned char *sd = stage + kTile * (8 + sizeof(T));
+  __shared__ unsigned cnt[256];
+  __shared__ unsigned tstart[256];
+  __shared__ int64_t gcur[256];
+  __shared__ unsigned wsum[kThreads / 32];
+  if ((int)blockIdx.x >= *nchunks_total) return;
+  const Chunk c = chunks[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  gcur[tid] = tid <= mask2 ? offs[count_index(c, tid)] : 0;
+  int64_t k[kPer];
+  T p[kPer];
+  auto load_tile = [&](int64_t t0) {
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      const int64_t i = t0 + j * kThreads + tid;
+      const bool valid = i < c.end;
+      k[j] = valid ? __ldg(q + i) : 0;
+      p[j] = valid ? payload_of<T, LOAD>(pay_in, c, i) : (T)0;
+    }
+  };
+  load_tile(c.begin);
+  for (int64_t t0 = c.begin; t0 < c.end; t0 += kTile) {
+    cnt[tid] = 0;
+    __syncthreads();
+    unsigned dr[kPer];  // digit << 16 | rank inside the tile's digit run; ~0u past the end
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      if (t0 + j * kThreads + tid < c.end) {
+        const unsigned d = (unsigned)((bk(k[j]) >> shift2) & mask2);
+        dr[j] = d << 16 | atomicAdd(&cnt[d], 1u);
+      } else {
+        dr[j] = ~0u;
+      }
+    }
+    __syncthreads();
+    // exclusive scan of the 256 tile counts (one per thread)
+    const unsigned mine = cnt[tid];
+    unsigned incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    unsigned before = incl - mine;
+    for (int x = 0; x < w; x++) before += wsum[x];
+    tstart[tid] = before;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      if (dr[j] != ~0u) {
+        const unsigned d = dr[j] >> 16;
+        const unsigned sl = tstart[d] + (dr[j] & 0xffffu);
+        sk[sl] = k[j];
+        sp[sl] = p[j];
+        sd[sl] = (unsigned char)d;
+      }
+    }
+    __syncthreads();
+    if (t0 + kTile < c.end) load_tile(t0 + kTile);  // the next tile's loads overlap the write-out
+    const int n = (int)min((int64_t)kTile, c.end - t0);
+    for (int sl = tid; sl < n; sl += kThreads) {
+      const int d = sd[sl];
+      const int64_t o = gcur[d] + (sl - (int)tstart[d]);
+      q_out[o] = sk[sl];
+      pay_out[o] = sp[sl];
+    }
+    __syncthreads();
+    gcur[tid] += cnt[tid];
+  }
+}
+
+// Inverse of one pass for 64-bit results: CTA per input chunk.  The chunk's
+// elements sit in one contiguous run per digit (offs gives the run starts, in
+// [bucket][digit][chunk] order, so the next entry ends the run); each carries
+// its offset inside the chunk.  The results are placed by offset in shared
+// memory, then written to the chunk's input range in order.
+__global__ void __launch_bounds__(kRevThreads) psa_unpermute_kernel(const Chunk *__restrict__ chunks,
+                                                                    const int32_t *__restrict__ nchunks_total,
+                                                                    const int64_t *__restrict__ offs, int nd,
+                                                                    const int64_t *__restrict__ res_in,
+                                                                    const uint16_t *__restrict__ loc,
+                                                                    int64_t *__restrict__ res_out) {
+  extern __shared__ __align__(16) int64_t staged[];  // kChunk results
+  __shared__ int64_t rs[256];
+  __shared__ int32_t pre[257];
+  __shared__ int32_t wsum[8];
+  if ((int)blockIdx.x >= *nchunks_total) return;
+  const Chunk c = chunks[blockIdx.x];
+  const int tid = threadIdx.x;
+  const int len = (int)(c.end - c.begin);
+  if (tid < 256) {  // run of digit tid: start and length; exclusive scan of the lengths
+    int32_t ln = 0;
+    if (tid < nd) {
+      const int64_t k = count_index(c, tid);
+      rs[tid] = offs[k];
+      ln = (int32_t)(offs[k + 1] - offs[k]);
+    }
+    int32_t incl = ln;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if ((tid & 31) >= o) incl += y;
+    }
+    if ((tid & 31) == 31) wsum[tid >> 5] = incl;
+    pre[tid] = incl - ln;  // within the warp, completed below
+  }
+  __syncthreads();
+  if (tid < 256) {
+    int32_t add = 0;
+    for (int x = 0; x < (tid >> 5); x++) add += wsum[x];
+    pre[tid] += add;
+  }
+  __syncthreads();
+  for (int f = tid; f < len; f += kRevThreads) {
+    int lo = 0, hi = nd - 1;  // the digit whose run holds flat index f: last d with pre[d] <= f
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pre[mid] <= f) {
+        lo = mid;
+      } else {
+        hi = mid - 1;
+      }
+    }
+    const int64_t j = rs[lo] + (f - pre[lo]);
+    staged[__ldg(loc + j)] = __ldg(res_in + j);
+  }
+  __syncthreads();
+  for (int x = tid; x < len; x += kRevThreads) res_out[c.begin + x] = staged[x];
+}
+
+// One CTA: chunk descriptors for a pass.  bstart == nullptr: the whole input
+// as one bucket (nb = 1).  Otherwise every bucket [bstart[b], bstart[b+1]) of nb is
+// split into chunks of at most kChunk queries; chunks are ordered by bucket.
+__global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__ bstart, int nb, int64_t n,
+                                                     Chunk *__restrict__ chunks, int32_t *__restrict__ nchunks_total) {
+  __shared__ int32_t pre[1024];
+  const int tid = threadIdx.x;
+  if (!bstart) {  // one bucket: the whole input
+    const int32_t nc = (int32_t)((n + kChunk - 1) / kChunk);
+    for (int32_t i = tid; i < nc; i += 1024) {
+      Chunk c;
+      c.begin = (int64_t)i * kChunk;
+      c.end = min(n, c.begin + kChunk);
+      c.bucket = 0;
+      c.idx = i;
+      c.nchunks = nc;
+      c.base = 0;
+      chunks[i] = c;
+    }
+    if (tid == 0) *nchunks_total = nc;
+    return;
+  }
+  const int per = (nb + 1023) / 1024;
+  int32_t mine = 0;
+  for (int x = 0; x < per; x++) {
+    const int b = tid * per + x;
+    if (b < nb) mine += (int32_t)((bstart[b + 1] - bstart[b] + kChunk - 1) / kChunk);
+  }
+  pre[tid] = mine;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan
+    const int32_t v = tid >= o ? pre[tid - o] : 0;
+    __syncthreads();
+    pre[tid] += v;
+    __syncthreads();
+  }
+  int32_t base = pre[tid] - mine;
+  for (int x = 0; x < per; x++) {
+    const int b = tid * per + x;
+    if (b >= nb) break;
+    const int64_t s = bstart[b], e = bstart[b + 1];
+    const int32_t nc = (int32_t)((e - s + kChunk - 1) / kChunk);
+    for (int32_t i = 0; i < nc; i++) {
+      Chunk c;
+      c.begin = s + (int64_t)i * kChunk;
+      c.end = min(e, c.begin + kChunk);
+      c.bucket = b;
+      c.idx = i;
+      c.nchunks = nc;
+      c.base = base;
+      chunks[base + i] = c;
+    }
+    base += nc;
+  }
+  if (tid == 1023) *nchunks_total = pre[1023];
+}
+
+// Starts of the pass's output buckets: bucket (b, d) starts at the offset of
+// digit d in b's first chunk; an empty input bucket b starts where it did.
+__global__ void bucket_starts_kernel(const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total,
+                                     const int64_t *__restrict__ offs, int nb, int nd, int64_t n,
+                                     const int64_t *__restrict__ bstart_in, int64_t *__restrict__ bstart) {
+  const int total = nb * nd;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x <= total; x += gridDim.x * blockDim.x) {
+    if (x == total) {
+      bstart[total] = n;
+      continue;
+    }
+    const int b = x / nd, d = x % nd;
+    int lo = 0, hi = *nchunks_total - 1, first = -1;
+    while (lo <= hi) {  // first chunk of bucket b
+      const int mid = (lo + hi) >> 1;
+      const int mb = chunks[mid].bucket;
+      if (mb < b) {
+        lo = mid + 1;
+      } else {
+        if (mb == b) first = mid;
+        hi = mid - 1;
+      }
+    }
+    bstart[x] = first >= 0 ? offs[count_index(chunks[first], d)] : (bstart_in ? bstart_in[b] : 0);
+  }
+}
+
+Bucket make_bucket(const hm_tree *t, int bits) {
+  Bucket d;
   d.lo = t->key_min;
   d.hi = t->key_max;
   d.maxd = (1 << bits) - 1;
@@ -47,40 +344,145 @@ KeyDigit make_digit(const hm_tree *t, int bits) {
   int len = 0;
   while (len < 64 && (range >> len) != 0) len++;
   d.shift = len > bits ? len - bits : 0;
-  d.sub_shift = 0;
-  d.sub_mask = 0xff;
   return d;
+}
+
+int64_t max_chunks(int64_t n, int nb) { return (n + kChunk - 1) / kChunk + nb + 1; }
+
+// One pass's chunk descriptors and scanned counts (kept for the inverse).
+struct Pass {
+  Chunk *chunks;
+  int32_t *nchunks;
+  int64_t *offs;  // 256 * mc + 1
+  int64_t mc;
+};
+
+struct Work {
+  Pass p1, p2;
+  void *scan;
+  int64_t *bstart1;  // first-pass bucket starts (257)
+  int64_t *bstart;   // final bucket starts (2^bits + 1)
+  int64_t *q_tmp;    // first-pass keys (two passes); the inverse's temporary
+  void *pay1;        // first-pass payloads (two passes)
+  uint16_t *loc;     // final offsets (offset mode)
+};
+
+size_t work_layout(int64_t n, int bits, bool offsets, Work *w, char *base) {
+  const bool two = bits > 8;
+  const int64_t mc1 = max_chunks(n, 1), mc2 = two ? max_chunks(n, 256) : 0;
+  const size_t pay = offsets ? 2 : 4;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char *p = base ? base + off : nullptr;
+    off += (size_t)align_up((int64_t)bytes, 256);
+    return p;
+  };
+  Work x{};
+  x.p1.mc = mc1;
+  x.p1.chunks = reinterpret_cast<Chunk *>(take(sizeof(Chunk) * mc1));
+  x.p1.nchunks = reinterpret_cast<int32_t *>(take(16));
+  x.p1.offs = reinterpret_cast<int64_t *>(take(8 * (256 * mc1 + 1)));
+  if (two) {
+    x.p2.mc = mc2;
+    x.p2.chunks = reinterpret_cast<Chunk *>(take(sizeof(Chunk) * mc2));
+    x.p2.nchunks = reinterpret_cast<int32_t *>(take(16));
+    x.p2.offs = reinterpret_cast<int64_t *>(take(8 * (256 * mc2 + 1)));
+  }
+  x.scan = take(scan_scratch_bytes(256 * std::max(mc1, mc2)));
+  x.bstart1 = reinterpret_cast<int64_t *>(take(8 * 258));
+  x.bstart = reinterpret_cast<int64_t *>(take(8 * (((size_t)1 << bits) + 1)));
+  x.q_tmp = two ? reinterpret_cast<int64_t *>(take(8 * n)) : nullptr;
+  x.pay1 = two ? take(pay * n) : nullptr;
+  x.loc = offsets ? reinterpret_cast<uint16_t *>(take(2 * n)) : nullptr;
+  if (w) *w = x;
+  return off;
+}
+
+template <typename T, bool LOAD>
+void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, const int64_t *bstart_in, int nb,
+              int shift2, int mask2, int64_t *q_out, T *pay_out, int64_t *bstart_out, const Pass &ps, void *scan,
+              cudaStream_t s) {
+  chunk_kernel<<<1, 1024, 0, s>>>(bstart_in, nb, n, ps.chunks, ps.nchunks);
+  cudaMemsetAsync(ps.offs, 0, sizeof(int64_t) * (256 * ps.mc + 1), s);
+  psa_hist_kernel<<<(unsigned)ps.mc, kThreads, 0, s>>>(q, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs);
+  exclusive_scan_i64(ps.offs, ps.offs, 256 * ps.mc, scan, s);
+  static bool attr_set = false;  // opt in to > 48 KiB of shared memory once
+  if (!attr_set) {
+    cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes<T>());
+    cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    attr_set = true;
+  }
+  psa_scatter_kernel<T, LOAD><<<(unsigned)ps.mc, kThreads, stage_bytes<T>(), s>>>(
+      q, pay_in, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs, q_out, pay_out);
+  const int nd = mask2 + 1;
+  bucket_starts_kernel<<<(unsigned)((nb * nd + 256) / 256), 256, 0, s>>>(ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
+                                                                         bstart_in, bstart_out);
+  note_launch(5);
+}
+
+void unpermute_pass(const Pass &ps, int nd, const int64_t *res_in, const uint16_t *loc, int64_t *res_out,
+                    cudaStream_t s) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(psa_unpermute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(8 * kChunk));
+    cudaFuncSetAttribute(psa_unpermute_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    attr_set = true;
+  }
+  psa_unpermute_kernel<<<(unsigned)ps.mc, kRevThreads, 8 * kChunk, s>>>(ps.chunks, ps.nchunks, ps.offs, nd, res_in,
+                                                                        loc, res_out);
+  note_launch();
 }
 
 }  // namespace
 
-size_t partition_scratch_bytes(int64_t n, int bits) {
-  size_t b = radix::pass_scratch_bytes(n);
-  if (bits > 8) b += (size_t)align_up(n * 8, 256) + (size_t)align_up(n * 4, 256);
-  return b;
+size_t partition_scratch_bytes(int64_t n, int bits, bool offsets) {
+  return work_layout(n, bits, offsets, nullptr, nullptr) + 256;
 }
 
-int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, int64_t *q_out,
-                      int32_t *pos_out, void *scratch, cudaStream_t s) {
-  if (bits < 1 || bits > 16 || n > INT32_MAX) return HM_EINVAL;
-  KeyDigit dg = make_digit(t, bits);
+int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, int64_t *q_out, int32_t *pos_out,
+                      void *scratch, cudaStream_t s, const int64_t **bucket_start) {
+  if (n == 0) return HM_OK;
+  if (bits < 1 || bits > 16 || n > INT32_MAX || n < 0) return HM_EINVAL;
+  const bool offsets = pos_out == nullptr;
+  Work w;
+  work_layout(n, bits, offsets, &w, static_cast<char *>(scratch));
+  const Bucket bk = make_bucket(t, bits);
   if (bits <= 8) {
-    dg.sub_mask = (1 << bits) - 1;
-    radix::stable_pass<int64_t, int32_t, KeyDigit, true>(q, nullptr, q_out, pos_out, n, dg, scratch, s);
-    return cuda_err(cudaGetLastError());
+    if (offsets)
+      one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, w.loc, w.bstart, w.p1,
+                                w.scan, s);
+    else
+      one_pass<int32_t, false>(bk, q, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, pos_out, w.bstart, w.p1,
+                               w.scan, s);
+  } else {
+    const int low = bits - 8;
+    if (offsets) {
+      uint16_t *loc1 = static_cast<uint16_t *>(w.pay1);
+      one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1, w.p1, w.scan, s);
+      one_pass<uint16_t, false>(bk, w.q_tmp, nullptr, n, w.bstart1, 256, 0, (1 << low) - 1, q_out, w.loc, w.bstart,
+                                w.p2, w.scan, s);
+    } else {
+      int32_t *pos1 = static_cast<int32_t *>(w.pay1);
+      one_pass<int32_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, pos1, w.bstart1, w.p1, w.scan, s);
+      one_pass<int32_t, true>(bk, w.q_tmp, pos1, n, w.bstart1, 256, 0, (1 << low) - 1, q_out, pos_out, w.bstart, w.p2,
+                              w.scan, s);
+    }
   }
-  // two stable passes: low (bits-8) bits of the bucket, then its high 8 bits
-  char *p = static_cast<char *>(scratch) + radix::pass_scratch_bytes(n);
-  int64_t *q_tmp = reinterpret_cast<int64_t *>(p);
-  int32_t *pos_tmp = reinterpret_cast<int32_t *>(p + align_up(n * 8, 256));
-  KeyDigit lo = dg;
-  lo.sub_shift = 0;
-  lo.sub_mask = (1 << (bits - 8)) - 1;
-  radix::stable_pass<int64_t, int32_t, KeyDigit, true>(q, nullptr, q_tmp, pos_tmp, n, lo, scratch, s);
-  KeyDigit hi = dg;
-  hi.sub_shift = bits - 8;
-  hi.sub_mask = 0xff;
-  radix::stable_pass<int64_t, int32_t, KeyDigit, false>(q_tmp, pos_tmp, q_out, pos_out, n, hi, scratch, s);
+  if (bucket_start) *bucket_start = w.bstart;
+  return cuda_err(cudaGetLastError());
+}
+
+int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, void *scratch, cudaStream_t s) {
+  if (n == 0) return HM_OK;
+  if (bits < 1 || bits > 16 || n > INT32_MAX || n < 0) return HM_EINVAL;
+  Work w;
+  work_layout(n, bits, true, &w, static_cast<char *>(scratch));
+  if (bits <= 8) {
+    unpermute_pass(w.p1, 1 << bits, res_sorted, w.loc, out, s);
+  } else {
+    unpermute_pass(w.p2, 1 << (bits - 8), res_sorted, w.loc, w.q_tmp, s);
+    unpermute_pass(w.p1, 256, w.q_tmp, static_cast<const uint16_t *>(w.pay1), out, s);
+  }
   return cuda_err(cudaGetLastError());
 }
 

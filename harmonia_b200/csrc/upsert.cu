@@ -76,21 +76,6 @@ __global__ void compact_batch_kernel(const uint64_t *__restrict__ uk, const int6
   }
 }
 
-__device__ __forceinline__ int32_t descend_to_leaf(const DevTree &t, int f, int64_t q) {
-  const int ix = f / 8, row = ix + f;
-  int32_t node = 0;
-  for (int l = 0; l < t.height; l++) {
-    const int64_t *r = t.inner + (int64_t)node * row;
-    int k = 0;
-    for (int v = 0; v < ix; v++) k += (r[v] <= q);
-    k = min(k, ix - 1);
-    int c = 8 * k;
-    for (int v = 0; v < 8; v++) c += (r[ix + 8 * k + v] <= q);
-    node = t.prefix[node] + c;
-  }
-  return node - t.n_inner;
-}
-
 // Hits are updated in place; misses get miss[i] = 1 and their leaf.
 __global__ void apply_kernel(DevTree t, int f, int lc, int li, int flags,
                              const int64_t *__restrict__ bk, const int64_t *__restrict__ bv, int64_t m,
@@ -99,7 +84,7 @@ __global__ void apply_kernel(DevTree t, int f, int lc, int li, int flags,
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
        i += (int64_t)gridDim.x * blockDim.x) {
     int64_t k = bk[i];
-    int32_t leaf = descend_to_leaf(t, f, k);
+    int32_t leaf = descend_leaf(t, f, k);
     const int64_t *kr = t.leaf_rows + (int64_t)leaf * (li + 2 * lc) + li;
     int cnt = t.leaf_cnt[leaf];
     int slot = -1;

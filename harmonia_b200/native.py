@@ -49,7 +49,7 @@ class Config(ctypes.Structure):
     _fields_ = [("fanout", ctypes.c_int), ("leaf_cap", ctypes.c_int), ("inner_fill", ctypes.c_int),
                 ("leaf_fill", ctypes.c_int), ("group_width", ctypes.c_int),
                 ("queries_per_group", ctypes.c_int), ("sort_bits", ctypes.c_int),
-                ("smem_bytes", ctypes.c_int), ("cache_hints", ctypes.c_int)]
+                ("smem_bytes", ctypes.c_int), ("cache_hints", ctypes.c_int), ("join", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -71,6 +71,9 @@ typedef struct {
   int smem_bytes;        /* budget for top levels staged in shared memory (default 49152) */
   int cache_hints;       /* L2 policy: 1 = inner rows evict_last, leaves evict_first; 2 = none
                             (default 1) */
+  int join;              /* large batches: 1 = pre-sort + bucket join, 2 = never, -1 = when the
+                            batch has at least half as many queries as the tree has leaves
+                            and 2^20 queries (default -1) */
 } hm_config;
 
 /* Read-only description of a loaded tree. */

@@ -28,10 +28,11 @@ def test_c2_point_full_size(big, fanout, leaf_cap):
     dq = torch.from_numpy(q).cuda()
     with BPlusTree.bulk_load(torch.from_numpy(keys).cuda(), torch.from_numpy(dg.values_for(keys)).cuda(),
                              fanout=fanout, leaf_cap=leaf_cap) as t:
-        for bits in (0, 8):
-            t.set_search_config(sort_bits=bits)
+        for bits, join in ((0, 2), (8, 2), (16, 2), (0, 1)):
+            t.set_search_config(sort_bits=bits, join=join)
             out = t.search(dq).cpu().numpy()
-            assert digest(out) == g["digest"], f"sort_bits={bits}"
+            assert digest(out) == g["digest"], f"sort_bits={bits} join={join}"
+        t.set_search_config(sort_bits=0, join=2)
         # the same batch partially sorted by its top 16 key bits: same results per key
         order = np.argsort(q >> np.int64(47), kind="stable")
         out = t.search(torch.from_numpy(q[order]).cuda()).cpu().numpy()

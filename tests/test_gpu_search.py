@@ -77,11 +77,11 @@ def test_every_group_width_and_depth(c1, w, qpg):
     keys, sk, t = c1
     q = dg.gen_point_queries(keys, 300001, 0.7, seed=w * 10 + qpg)
     exp = po.PortTree(sk, dg.values_for(sk)).search(q)
-    t.set_search_config(group_width=w, queries_per_group=qpg, sort_bits=0)
+    t.set_search_config(group_width=w, queries_per_group=qpg, sort_bits=0, join=2)
     try:
         assert (t.search(cuda(q)).cpu().numpy() == exp).all()
     finally:
-        t.set_search_config(group_width=4, queries_per_group=2, sort_bits=-1)
+        t.set_search_config(group_width=4, queries_per_group=2, sort_bits=-1, join=-1)
 
 
 @pytest.mark.parametrize("bits", [1, 4, 8, 9, 12, 16])
@@ -89,11 +89,11 @@ def test_presort_bits(c1, bits):
     keys, sk, t = c1
     q = dg.gen_point_queries(keys, 1 << 19, 0.9, seed=bits)
     exp = po.PortTree(sk, dg.values_for(sk)).search(q)
-    t.set_search_config(sort_bits=bits)
+    t.set_search_config(sort_bits=bits, join=2)
     try:
         assert (t.search(cuda(q)).cpu().numpy() == exp).all()
     finally:
-        t.set_search_config(sort_bits=-1)
+        t.set_search_config(sort_bits=-1, join=-1)
 
 
 @pytest.mark.parametrize("fanout,leaf_cap", CONFIGS)
@@ -230,3 +230,45 @@ def test_plan_replay_matches_and_follows_rebuild():
         for q, o in zip(qs, outs):
             assert (o.cpu().numpy() == exp.search(q.cpu().numpy())).all()
         plan.close()
+
+
+@pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (128, 64)])
+def test_bucket_join_matches_oracle(fanout, leaf_cap):
+    keys = dg.gen_keys(1 << 20, seed=81)
+    sk = np.sort(keys)
+    oracle = po.PortTree(sk, dg.values_for(sk))
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), fanout=fanout, leaf_cap=leaf_cap) as t:
+        t.set_search_config(join=1)
+        q = dg.gen_point_queries(keys, (1 << 21) + 333, 0.7, seed=82)
+        q[:6] = [sk[0], sk[-1], sk[0] - 1, sk[-1] + 1, -(2**63), 2**63 - 1]
+        assert (t.search(cuda(q)).cpu().numpy() == oracle.search(q)).all()
+        z = dg.gen_zipf_queries(sk, 1 << 21, 0.99, seed=83)  # hot buckets split into several runs
+        assert (t.search(cuda(z)).cpu().numpy() == oracle.search(z)).all()
+        t.set_search_config(join=-1)
+
+
+@pytest.mark.parametrize("ends", [(-(2**62), 2**62), (-(2**63), 2**63 - 2), (2**40, 2**63 - 2)])
+def test_bucket_join_skewed_keys_fall_back(ends):
+    # almost all keys in a narrow range: buckets over it hold too many leaves;
+    # extreme ends put bucket boundaries past the largest key
+    rng = np.random.default_rng(5)
+    dense = np.unique(rng.integers(10**12, 10**12 + 10**8, 1 << 20))
+    keys = np.unique(np.concatenate([dense, np.array(ends, np.int64)])).astype(np.int64)
+    rng.shuffle(keys)
+    sk = np.sort(keys)
+    oracle = po.PortTree(sk, dg.values_for(sk))
+    with BPlusTree.bulk_load(keys, dg.values_for(keys)) as t:
+        t.set_search_config(join=1)
+        q = np.concatenate([sk[rng.integers(0, len(sk), 1 << 20)], rng.integers(10**12, 10**12 + 10**8, 1 << 19)])
+        assert (t.search(cuda(q)).cpu().numpy() == oracle.search(q)).all()
+
+
+def test_bucket_join_after_upserts(c1):
+    keys, sk, _ = c1
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), leaf_fill=12) as t:
+        bk, bv = dg.gen_upserts(keys, 5000, 0.5, seed=91)
+        t.upsert(bk, bv)
+        ek, ev = po.upsert_set(sk, dg.values_for(sk), bk, bv)
+        q = np.concatenate([bk, dg.gen_point_queries(ek, 1 << 20, 0.8, seed=92)])
+        t.set_search_config(join=1)
+        assert (t.search(cuda(q)).cpu().numpy() == po.PortTree(ek, ev).search(q)).all()
