@@ -432,24 +432,33 @@ def main():
     tree.profile(False)
     value = replicas.job_throughput(m, ws, ms)  # Mqueries/s (m queries per rank per step)
 
-    search_launches, search_total = stages.get("search", (0, 0.0))
-    search_ms = search_total / max(search_launches, 1)
     peak, peak_kind = peaks()
-    bq = algorithmic_bytes_per_query(args.fanout)
-    achieved = bq * m / (search_ms * 1e-3) / 1e9 if search_ms > 0 else None
+    info = tree.info()
+    if stages.get("join"):
+        # the bucket join dominates: it reads every query (8 B), writes every
+        # result (8 B) and stages every leaf record once
+        kernel, stage_key = "join_kernel", "join"
+        bq = 16 + info.n_leaf * info.leaf_row_words * 8 / m
+    else:
+        kernel, stage_key = "search_kernel", "search"
+        bq = algorithmic_bytes_per_query(args.fanout)
+    k_launches, k_total = stages.get(stage_key, (0, 0.0))
+    kernel_ms = k_total / max(k_launches, 1)
+    achieved = bq * m / (kernel_ms * 1e-3) / 1e9 if kernel_ms > 0 else None
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            key = "join" if stages.get("join") else f"bits{tuned['sort_bits']}"
+            key = "join" if kernel == "join_kernel" else f"bits{tuned['sort_bits']}"
             traffic = json.load(open(tf)).get(f"search_f{args.fanout}_lc{args.leaf_cap}_{key}")
         except Exception:
             traffic = None
-    roofline = {"bound": "hbm", "kernel": "search_kernel", "achieved": round(achieved, 1) if achieved else None,
+    roofline = {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1) if achieved else None,
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
                 "peak_kind": peak_kind, "traffic": traffic,
-                "algorithmic_bytes_per_query": bq, "queries_per_launch": m,
-                "kernel_ms": round(search_ms, 4)}
+                "algorithmic_bytes_per_query": round(bq, 2), "queries_per_launch": m,
+                "kernel_ms": round(kernel_ms, 4),
+                "path_ms": round(sum(v[1] / max(v[0], 1) for v in stages.values()), 4)}
 
     # pre-sorted input (the batch arrives partially sorted by its top 16 key bits)
     if args.extras:

@@ -31,7 +31,17 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kPerThread = 4;
 constexpr int kRun = kThreads * kPerThread;  // queries per work item
-constexpr int kStageMax = 96 * 1024;         // shared memory of one stage, at most
+#ifndef HM_JOIN_STAGES
+#define HM_JOIN_STAGES 2  // shared-memory ring of the join kernel
+#endif
+#ifndef HM_JOIN_MINB
+#define HM_JOIN_MINB 4  // resident join CTAs per SM the register budget allows
+#endif
+#ifndef HM_JOIN_SLACK
+#define HM_JOIN_SLACK 4  // a stage holds mean + mean / HM_JOIN_SLACK + 8 leaves
+#endif
+constexpr int kStages = HM_JOIN_STAGES;
+constexpr int kStageMax = (216 / kStages) * 1024;  // shared memory of one stage, at most
 
 // A work item: a run of at most kRun queries of one bucket and the bucket's
 // leaves [l0, l0 + nl).
@@ -96,7 +106,6 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Words of one leaf in a stage: its keys at a stride of LC + 1 (leaf m's key s
@@ -165,16 +174,18 @@ __device__ __noinline__ int64_t lookup_scalar(const DevTree &t, int f, int64_t q
   return v;
 }
 
-// Persistent CTAs walk the items with a stride of the grid; two stages: the
-// leaves of the next item are copied (cp.async) while the current one is
-// answered from shared memory.  Item descriptors and the queries of the next
-// item are loaded one iteration ahead.  Results are written in the grouped
-// order (out[i] for grouped query i).
+// Persistent CTAs walk the items with a stride of the grid through a ring of
+// kStages shared-memory stages: the leaves of the next kStages - 1 items are
+// in flight (cp.async) while the current one is answered from shared memory.
+// Item descriptors are loaded kStages items ahead and the queries of the next
+// item one item ahead.  Results are written in the grouped order (out[i] for
+// grouped query i).
 template <int LC>
-__global__ void __launch_bounds__(kThreads, 4) join_kernel(DevTree t, int f, const Item *__restrict__ items,
+__global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t, int f, const Item *__restrict__ items,
                                                         const int64_t *__restrict__ nitems,
                                                         const int64_t *__restrict__ qs, int64_t *__restrict__ out,
                                                         int ml) {
+  static_assert(kStages >= 2, "a ring of at least two stages");
   extern __shared__ __align__(16) int64_t smem[];
   const int stage_words = ml * (2 * LC + 1);
   const int64_t n_items = *nitems;
@@ -182,30 +193,36 @@ __global__ void __launch_bounds__(kThreads, 4) join_kernel(DevTree t, int f, con
   int64_t it = blockIdx.x;
   if (it >= n_items) return;
   const Item none{0, 0, 0, 0};
-  Item cur = items[it];
-  Item nxt = it + g < n_items ? items[it + g] : none;
-  stage_leaves<LC>(t, cur, Stage<LC>(smem, ml), ml);
-  cp_async_commit();
+  Item d[kStages];  // items it, it + g, ..., it + (kStages - 1) g
+#pragma unroll
+  for (int x = 0; x < kStages; x++) d[x] = it + x * g < n_items ? items[it + x * g] : none;
+#pragma unroll
+  for (int x = 0; x < kStages - 1; x++) {
+    stage_leaves<LC>(t, d[x], Stage<LC>(smem + x * stage_words, ml), ml);
+    cp_async_commit();
+  }
   int64_t q[kPerThread];
 #pragma unroll
   for (int j = 0; j < kPerThread; j++) {
     const int r = j * kThreads + threadIdx.x;
-    q[j] = r < cur.len ? __ldg(qs + cur.qa + r) : 0;
+    q[j] = r < d[0].len ? __ldg(qs + d[0].qa + r) : 0;
   }
-  for (int k = 0; it < n_items; k++, it += g) {
-    Stage<LC> st(smem + (k & 1) * stage_words, ml);
-    // next item: its leaves into the other stage, its descriptor after it
-    stage_leaves<LC>(t, nxt, Stage<LC>(smem + ((k + 1) & 1) * stage_words, ml), ml);
+  int cur_stage = 0;
+  for (; it < n_items; it += g) {
+    const int fill = cur_stage == 0 ? kStages - 1 : cur_stage - 1;  // (cur + kStages - 1) % kStages
+    stage_leaves<LC>(t, d[kStages - 1], Stage<LC>(smem + fill * stage_words, ml), ml);
     cp_async_commit();
-    const Item after = it + 2 * g < n_items ? items[it + 2 * g] : none;
+    const Item dn = it + kStages * g < n_items ? items[it + kStages * g] : none;
     int64_t qn[kPerThread];
 #pragma unroll
     for (int j = 0; j < kPerThread; j++) {
       const int r = j * kThreads + threadIdx.x;
-      qn[j] = r < nxt.len ? __ldg(qs + nxt.qa + r) : 0;
+      qn[j] = r < d[1].len ? __ldg(qs + d[1].qa + r) : 0;
     }
-    cp_async_wait_prev();
+    asm volatile("cp.async.wait_group %0;" ::"n"(kStages - 1) : "memory");  // the current item's group is done
     __syncthreads();
+    const Item cur = d[0];
+    const Stage<LC> st(smem + cur_stage * stage_words, ml);
     const bool staged = cur.nl >= 1 && cur.nl <= ml;
     int span = 1;
     while (span < cur.nl) span <<= 1;
@@ -217,11 +234,13 @@ __global__ void __launch_bounds__(kThreads, 4) join_kernel(DevTree t, int f, con
       if (q[j] != kMaxKey) v = staged ? lookup_staged<LC>(st, cur.nl, span, q[j]) : lookup_scalar<LC>(t, f, q[j]);
       out[cur.qa + r] = v;  // grouped order: consecutive threads, consecutive slots
     }
-    __syncthreads();  // the stage is refilled two items later
-    cur = nxt;
-    nxt = after;
+    __syncthreads();  // this stage is refilled in the next iteration
+#pragma unroll
+    for (int x = 0; x < kStages - 1; x++) d[x] = d[x + 1];
+    d[kStages - 1] = dn;
 #pragma unroll
     for (int j = 0; j < kPerThread; j++) q[j] = qn[j];
+    cur_stage = cur_stage == kStages - 1 ? 0 : cur_stage + 1;
   }
   cp_async_wait_all();
 }
@@ -230,11 +249,12 @@ int64_t max_items(int64_t n, int nb) { return n / kRun + nb + 1; }
 
 int leaf_bytes(int lc) { return lc == 16 ? stage_leaf_bytes<16>() : stage_leaf_bytes<64>(); }
 
-// Leaves one stage holds: room for 1.5x the mean leaves per bucket plus a
-// margin, as an even count (keeps the value part 16-B aligned).
+// Leaves one stage holds: room for the mean leaves per bucket, a quarter more
+// and a margin, as an even count (keeps the value part 16-B aligned).  A
+// bucket of more leaves takes the scalar path.
 int stage_leaves_for(const hm_tree *t, int bits) {
   const int64_t mean = (t->n_leaf + ((int64_t)1 << bits) - 1) >> bits;
-  int64_t ml = mean + mean / 2 + 8;
+  int64_t ml = mean + mean / HM_JOIN_SLACK + 8;
   ml = std::min<int64_t>(ml, kStageMax / leaf_bytes(t->cfg.leaf_cap));
   return (int)(ml & ~int64_t(1));
 }
@@ -252,7 +272,7 @@ bool join_fits(const hm_tree *t) {
   if (t->cfg.leaf_cap != 16 && t->cfg.leaf_cap != 64) return false;
   const int bits = join_bits(t);
   const int64_t mean = (t->n_leaf + ((int64_t)1 << bits) - 1) >> bits;
-  return mean + mean / 2 + 8 <= stage_leaves_for(t, bits) + 1;
+  return mean + mean / HM_JOIN_SLACK + 8 <= stage_leaves_for(t, bits) + 1;
 }
 
 size_t join_scratch_bytes(int64_t n, int bits) {
@@ -288,13 +308,13 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
   expand_items_kernel<<<gb, 256, 0, s>>>(nb, bstart, leafb, cnt, first, items);
   const int lc = t->cfg.leaf_cap;
   const int ml = stage_leaves_for(t, bits);
-  const size_t smem = (size_t)2 * ml * leaf_bytes(lc);
+  const size_t smem = (size_t)kStages * ml * leaf_bytes(lc);
   const int per_sm = std::max(1, std::min(8, (int)((227 * 1024) / (smem + 1024))));
   const unsigned grid = (unsigned)std::min<int64_t>(max_items(n, nb), (int64_t)t->num_sms * per_sm);
   static bool attr_set = false;  // opt in to > 48 KiB of shared memory once
   if (!attr_set) {
-    cudaFuncSetAttribute(join_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kStageMax);
-    cudaFuncSetAttribute(join_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kStageMax);
+    cudaFuncSetAttribute(join_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStages * kStageMax);
+    cudaFuncSetAttribute(join_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStages * kStageMax);
     cudaFuncSetAttribute(join_kernel<16>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(join_kernel<64>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     attr_set = true;

@@ -17,8 +17,9 @@
 //     second pass partitions every first-pass bucket on its own, in chunks that
 //     never straddle a bucket, with offsets from one global scan of counts laid
 //     out as [bucket][digit][chunk];
-//   * each pass stages a 4096-query tile in shared memory grouped by digit and
-//     writes it out so consecutive threads store consecutive slots;
+//   * each pass stages a 4096-query tile in shared memory grouped by digit
+//     (one 16-B slot per query: key, digit and payload) and writes it out so
+//     consecutive threads store consecutive slots;
 //   * the payload is either the query's input position (int32, for callers
 //     that scatter results themselves) or its offset inside its 8192-query
 //     input chunk (uint16).  With offsets, unpermute_results undoes the passes
@@ -38,7 +39,21 @@ constexpr int kThreads = 256;
 constexpr int kTile = 4096;
 constexpr int kPer = kTile / kThreads;
 constexpr int64_t kChunk = 8192;  // queries per CTA chunk (a multiple of kTile; offsets fit 16 bits)
-constexpr int kRevThreads = 512;
+
+// Launch shapes (compile-time tunables, measured on B200 at 2^24 queries).
+#ifndef HM_PSA_SCATTER_MINB
+#define HM_PSA_SCATTER_MINB 3  // resident scatter CTAs per SM the register budget allows
+#endif
+#ifndef HM_PSA_REV_THREADS
+#define HM_PSA_REV_THREADS 512
+#endif
+#ifndef HM_PSA_REV_MINB
+#define HM_PSA_REV_MINB 3
+#endif
+#ifndef HM_PSA_REV_BATCH
+#define HM_PSA_REV_BATCH 2  // digit runs a warp of the inverse reads at once
+#endif
+constexpr int kRevThreads = HM_PSA_REV_THREADS;
 
 // Bucket of a key: top `bits` bits of (k - lo) over the tree's key range.
 struct Bucket {
@@ -107,22 +122,20 @@ __device__ __forceinline__ T payload_of(const T *__restrict__ pay_in, const Chun
 
 template <typename T>
 constexpr int stage_bytes() {
-  return kTile * (8 + (int)sizeof(T) + 1);  // staged keys, payloads, digits
+  return kTile * 16;  // one 16-B slot per staged element: key, then digit << 32 | payload
 }
 
 template <typename T, bool LOAD>
-__global__ void __launch_bounds__(kThreads, 3) psa_scatter_kernel(const int64_t *__restrict__ q, const T *__restrict__ pay_in,
+__global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_kernel(const int64_t *__restrict__ q, const T *__restrict__ pay_in,
                                                            const Chunk *__restrict__ chunks,
                                                            const int32_t *__restrict__ nchunks_total, Bucket bk,
                                                            int shift2, int mask2, const int64_t *__restrict__ offs,
                                                            int64_t *__restrict__ q_out, T *__restrict__ pay_out) {
-  extern __shared__ __align__(16) unsigned char stage[];  // stage_bytes<T>(), dynamic
-  int64_t *sk = reinterpret_cast<int64_t *>(stage);
-  T *sp = reinterpret_cast<T *>(stage + kTile * 8);
-  unsigned char *sd = stage + kTile * (8 + sizeof(T));
+  extern __shared__ __align__(16) longlong2 slot[];  // kTile staged elements, dynamic
   __shared__ unsigned cnt[256];
   __shared__ unsigned tstart[256];
   __shared__ int64_t gcur[256];
+  __shared__ int64_t adj[256];
   __shared__ unsigned wsum[kThreads / 32];
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
@@ -167,25 +180,24 @@ __global__ void __launch_bounds__(kThreads, 3) psa_scatter_kernel(const int64_t 
     unsigned before = incl - mine;
     for (int x = 0; x < w; x++) before += wsum[x];
     tstart[tid] = before;
+    adj[tid] = gcur[tid] - (int64_t)before;  // slot sl of digit d goes to adj[d] + sl
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
       if (dr[j] != ~0u) {
         const unsigned d = dr[j] >> 16;
         const unsigned sl = tstart[d] + (dr[j] & 0xffffu);
-        sk[sl] = k[j];
-        sp[sl] = p[j];
-        sd[sl] = (unsigned char)d;
+        slot[sl] = make_longlong2(k[j], (long long)((uint64_t)d << 32 | (uint32_t)p[j]));
       }
     }
     __syncthreads();
     if (t0 + kTile < c.end) load_tile(t0 + kTile);  // the next tile's loads overlap the write-out
     const int n = (int)min((int64_t)kTile, c.end - t0);
     for (int sl = tid; sl < n; sl += kThreads) {
-      const int d = sd[sl];
-      const int64_t o = gcur[d] + (sl - (int)tstart[d]);
-      q_out[o] = sk[sl];
-      pay_out[o] = sp[sl];
+      const longlong2 e = slot[sl];
+      const int64_t o = adj[(uint64_t)e.y >> 32] + sl;
+      q_out[o] = e.x;
+      pay_out[o] = (T)(uint32_t)e.y;
     }
     __syncthreads();
     gcur[tid] += cnt[tid];
@@ -196,56 +208,58 @@ __global__ void __launch_bounds__(kThreads, 3) psa_scatter_kernel(const int64_t 
 // elements sit in one contiguous run per digit (offs gives the run starts, in
 // [bucket][digit][chunk] order, so the next entry ends the run); each carries
 // its offset inside the chunk.  The results are placed by offset in shared
-// memory, then written to the chunk's input range in order.
-__global__ void __launch_bounds__(kRevThreads) psa_unpermute_kernel(const Chunk *__restrict__ chunks,
-                                                                    const int32_t *__restrict__ nchunks_total,
-                                                                    const int64_t *__restrict__ offs, int nd,
-                                                                    const int64_t *__restrict__ res_in,
-                                                                    const uint16_t *__restrict__ loc,
-                                                                    int64_t *__restrict__ res_out) {
+// memory, then written to the chunk's input range in order.  A warp reads
+// whole runs (a lane per element, so every load is one coalesced request),
+// kRevBatch runs at a time with all their loads issued before the stores.
+constexpr int kRevWarps = kRevThreads / 32;
+constexpr int kRevBatch = HM_PSA_REV_BATCH;
+
+__global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_kernel(
+    const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total, const int64_t *__restrict__ offs,
+    int nd, const int64_t *__restrict__ res_in, const uint16_t *__restrict__ loc, int64_t *__restrict__ res_out) {
   extern __shared__ __align__(16) int64_t staged[];  // kChunk results
   __shared__ int64_t rs[256];
-  __shared__ int32_t pre[257];
-  __shared__ int32_t wsum[8];
+  __shared__ int32_t rl[256];
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int len = (int)(c.end - c.begin);
-  if (tid < 256) {  // run of digit tid: start and length; exclusive scan of the lengths
-    int32_t ln = 0;
-    if (tid < nd) {
-      const int64_t k = count_index(c, tid);
-      rs[tid] = offs[k];
-      ln = (int32_t)(offs[k + 1] - offs[k]);
-    }
-    int32_t incl = ln;
+  for (int d = tid; d < nd; d += kRevThreads) {  // run of digit d: start and length
+    const int64_t k = count_index(c, d);
+    const int64_t a = offs[k];
+    rs[d] = a;
+    rl[d] = (int32_t)(offs[k + 1] - a);
+  }
+  __syncthreads();
+  for (int d0 = wid; d0 < nd; d0 += kRevWarps * kRevBatch) {
+    int64_t r[kRevBatch][2];
+    uint16_t l[kRevBatch][2];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-      if ((tid & 31) >= o) incl += y;
-    }
-    if ((tid & 31) == 31) wsum[tid >> 5] = incl;
-    pre[tid] = incl - ln;  // within the warp, completed below
-  }
-  __syncthreads();
-  if (tid < 256) {
-    int32_t add = 0;
-    for (int x = 0; x < (tid >> 5); x++) add += wsum[x];
-    pre[tid] += add;
-  }
-  __syncthreads();
-  for (int f = tid; f < len; f += kRevThreads) {
-    int lo = 0, hi = nd - 1;  // the digit whose run holds flat index f: last d with pre[d] <= f
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (pre[mid] <= f) {
-        lo = mid;
-      } else {
-        hi = mid - 1;
+    for (int x = 0; x < kRevBatch; x++) {  // the first 64 elements of kRevBatch runs
+      const int d = d0 + x * kRevWarps;
+      const int n = d < nd ? rl[d] : 0;
+      const int64_t a = d < nd ? rs[d] : 0;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int e = lane + 32 * h;
+        if (e < n) {
+          r[x][h] = __ldg(res_in + a + e);
+          l[x][h] = __ldg(loc + a + e);
+        }
       }
     }
-    const int64_t j = rs[lo] + (f - pre[lo]);
-    staged[__ldg(loc + j)] = __ldg(res_in + j);
+#pragma unroll
+    for (int x = 0; x < kRevBatch; x++) {
+      const int d = d0 + x * kRevWarps;
+      const int n = d < nd ? rl[d] : 0;
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+        if (lane + 32 * h < n) staged[l[x][h]] = r[x][h];
+      if (n > 64) {  // a long run: the rest, a warp-wide step at a time
+        const int64_t a = rs[d];
+        for (int e = 64 + lane; e < n; e += 32) staged[__ldg(loc + a + e)] = __ldg(res_in + a + e);
+      }
+    }
   }
   __syncthreads();
   for (int x = tid; x < len; x += kRevThreads) res_out[c.begin + x] = staged[x];
