@@ -25,13 +25,25 @@ int scan_ctas(int64_t n) {
   return (int)c;
 }
 
+constexpr int kScanPer = 8;                    // elements per thread per scan step
+constexpr int kScanStep = kThreads * kScanPer;  // elements per CTA per scan step
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) seg_sum_kernel(const T *__restrict__ in, int64_t n,
                                                            int64_t seg, int64_t *__restrict__ part) {
   __shared__ int64_t red[kThreads / 32];
   int64_t b0 = (int64_t)blockIdx.x * seg, b1 = min(n, b0 + seg);
   int64_t s = 0;
-  for (int64_t i = b0 + threadIdx.x; i < b1; i += kThreads) s += (int64_t)in[i];
+  for (int64_t base = b0; base < b1; base += kScanStep) {
+    T v[kScanPer];
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) {  // all loads first
+      const int64_t i = base + j * kThreads + threadIdx.x;
+      v[j] = i < b1 ? in[i] : (T)0;
+    }
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) s += (int64_t)v[j];
+  }
   for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
@@ -42,35 +54,60 @@ __global__ void __launch_bounds__(kThreads) seg_sum_kernel(const T *__restrict__
   }
 }
 
-// Exclusive scan of each segment, offset by the scanned segment sums.
+// Exclusive scan of each segment, offset by the scanned segment sums.  A step
+// stages kScanStep elements in shared memory (coalesced), each thread scans
+// kScanPer consecutive ones (index i at i + i / 8: one pad word per 8 keeps
+// the threads' runs in different banks), one block scan of the thread sums.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) seg_scan_kernel(const T *__restrict__ in, int64_t n,
                                                             int64_t seg, const int64_t *__restrict__ part,
                                                             int64_t *__restrict__ out, int nctas) {
+  __shared__ int64_t buf[kScanStep + kScanStep / 8];
   __shared__ int64_t wsum[kThreads / 32];
   __shared__ int64_t carry;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int64_t b0 = (int64_t)blockIdx.x * seg, b1 = min(n, b0 + seg);
-  if (threadIdx.x == 0) carry = part[blockIdx.x];
-  __syncthreads();
-  for (int64_t t0 = b0; t0 < b1; t0 += kThreads) {
-    int64_t i = t0 + threadIdx.x;
-    int64_t v = i < b1 ? (int64_t)in[i] : 0;
-    int64_t x = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      int64_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+  if (tid == 0) carry = part[blockIdx.x];
+  for (int64_t base = b0; base < b1; base += kScanStep) {
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) {
+      const int e = j * kThreads + tid;
+      const int64_t i = base + e;
+      buf[e + (e >> 3)] = i < b1 ? (int64_t)in[i] : 0;
     }
-    if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    int64_t before = carry;
-    for (int w = 0; w < warp; w++) before += wsum[w];
-    if (i < b1) out[i] = before + x - v;
+    int64_t x[kScanPer], local = 0;
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) {
+      x[j] = buf[tid * (kScanPer + 1) + j];
+      local += x[j];
+    }
+    int64_t incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
     __syncthreads();
-    if (threadIdx.x == kThreads - 1) carry = before + x;
+    int64_t run = carry + incl - local;
+    for (int w = 0; w < warp; w++) run += wsum[w];
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) {
+      buf[tid * (kScanPer + 1) + j] = run;
+      run += x[j];
+    }
+    __syncthreads();
+    if (tid == kThreads - 1) carry = run;
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) {
+      const int e = j * kThreads + tid;
+      const int64_t i = base + e;
+      if (i < b1) out[i] = buf[e + (e >> 3)];
+    }
     __syncthreads();
   }
-  if (blockIdx.x == nctas - 1 && threadIdx.x == 0) out[n] = carry;
+  if (blockIdx.x == nctas - 1 && tid == 0) out[n] = carry;
 }
 
 __global__ void export_kernel(DevTree t, int lc, int li, int64_t *__restrict__ keys,

@@ -36,8 +36,12 @@ namespace hm {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kTile = 4096;
+#ifndef HM_PSA_TILE
+#define HM_PSA_TILE 4096  // queries a scatter CTA stages at a time
+#endif
+constexpr int kTile = HM_PSA_TILE;
 constexpr int kPer = kTile / kThreads;
+static_assert(kTile % kThreads == 0 && kTile <= 65536, "ranks are kept in 16 bits");
 constexpr int64_t kChunk = 8192;  // queries per CTA chunk (a multiple of kTile; offsets fit 16 bits)
 
 // Launch shapes (compile-time tunables, measured on B200 at 2^24 queries).
