@@ -215,8 +215,9 @@ SearchPlan plan_search(const hm_tree *t, int64_t n) {
   if (n <= 0 || n > INT32_MAX) return p;  // positions are carried as int32
   const hm_config &c = t->cfg;
   const bool join = (c.join == 1 && (c.leaf_cap == 16 || c.leaf_cap == 64)) ||
-                    (c.join == -1 && n >= std::max<int64_t>((int64_t)1 << 22, 4 * (int64_t)t->n_leaf) &&
-                     t->n_leaf >= 1024 && join_fits(t));  // measured: wins from ~4 queries per leaf
+                    (c.join == -1 && t->n_leaf >= 1024 && join_fits(t) &&
+                     // measured: the join wins from about 4 queries per leaf
+                     n >= std::min(t->join_tuned_min, std::max<int64_t>((int64_t)1 << 22, 4 * (int64_t)t->n_leaf)));
   if (join) {
     p.join = true;
     p.bits = join_bits(t);
@@ -751,11 +752,12 @@ int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n_, hm_config *best)
           cands.push_back(c);
         }
   {
-    hm_config c = orig;  // the bucket join (its own bucket bits)
+    hm_config c = orig;  // the bucket join (its own bucket bits), timed last
     c.join = 1;
     cands.push_back(c);
   }
   int rc = HM_OK;
+  float join_ms = 1e30f;
   for (const hm_config &c : cands) {
     t->cfg = c;
     choose_smem_levels(t);
@@ -772,10 +774,20 @@ int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n_, hm_config *best)
       if (rep > 0 && x < ms) ms = x;
     }
     if (rc) break;
-    if (ms < best_ms) {
+    if (c.join == 1) {
+      join_ms = ms;
+    } else if (ms < best_ms) {
       best_ms = ms;
       best_cfg = c;
     }
+  }
+  // The descent settings serve every batch; the join, where it won, serves
+  // batches at least as large as the sample (the automatic choice).
+  if (join_ms < best_ms) {
+    best_cfg.join = -1;
+    t->join_tuned_min = std::min<int64_t>(t->join_tuned_min, n);
+  } else {
+    best_cfg.join = 2;
   }
   t->cfg = rc ? orig : best_cfg;
   choose_smem_levels(t);

@@ -112,6 +112,7 @@ struct hm_tree {
   int num_sms = 148;
   int64_t key_min = 0, key_max = 0;  // for the pre-sort digit
   uint64_t generation = 0;           // bumped when the arena is rebuilt
+  int64_t join_tuned_min = INT64_MAX;  // smallest batch the autotuner saw the join win
   // arena
   void *arena = nullptr;
   size_t arena_bytes = 0;

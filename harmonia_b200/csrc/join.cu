@@ -30,7 +30,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kPerThread = 4;
-constexpr int kRun = kThreads * kPerThread;  // queries per work item
+constexpr int kRun = kThreads * kPerThread;  // queries a CTA answers per step
+constexpr int kItemRuns = 16;
+constexpr int kItemMax = kRun * kItemRuns;  // queries per work item, at most
 #ifndef HM_JOIN_STAGES
 #define HM_JOIN_STAGES 2  // shared-memory ring of the join kernel
 #endif
@@ -43,8 +45,8 @@ constexpr int kRun = kThreads * kPerThread;  // queries per work item
 constexpr int kStages = HM_JOIN_STAGES;
 constexpr int kStageMax = (216 / kStages) * 1024;  // shared memory of one stage, at most
 
-// A work item: a run of at most kRun queries of one bucket and the bucket's
-// leaves [l0, l0 + nl).
+// A work item: at most kItemMax queries of one bucket and the bucket's leaves
+// [l0, l0 + nl); the leaves are staged once for all of them.
 struct __align__(16) Item {
   int32_t qa, len, l0, nl;
 };
@@ -56,7 +58,7 @@ __global__ void bucket_prep_kernel(DevTree t, int f, int64_t lo, int shift, int 
                                    const int64_t *__restrict__ bstart, int32_t *__restrict__ leafb,
                                    int32_t *__restrict__ cnt) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x) {
-    cnt[b] = b < nb ? (int32_t)((bstart[b + 1] - bstart[b] + kRun - 1) / kRun) : 0;
+    cnt[b] = b < nb ? (int32_t)((bstart[b + 1] - bstart[b] + kItemMax - 1) / kItemMax) : 0;
     if (b == 0) {
       leafb[0] = 0;
       continue;
@@ -86,8 +88,8 @@ __global__ void expand_items_kernel(int nb, const int64_t *__restrict__ bstart, 
     int64_t o = first[b];
     for (int r = 0; r < c; r++) {
       Item it;
-      it.qa = (int32_t)(s + (int64_t)r * kRun);
-      it.len = (int32_t)min((int64_t)kRun, e - (s + (int64_t)r * kRun));
+      it.qa = (int32_t)(s + (int64_t)r * kItemMax);
+      it.len = (int32_t)min((int64_t)kItemMax, e - (s + (int64_t)r * kItemMax));
       it.l0 = l0;
       it.nl = nl;
       items[o + r] = it;
@@ -176,10 +178,10 @@ __device__ __noinline__ int64_t lookup_scalar(const DevTree &t, int f, int64_t q
 
 // Persistent CTAs walk the items with a stride of the grid through a ring of
 // kStages shared-memory stages: the leaves of the next kStages - 1 items are
-// in flight (cp.async) while the current one is answered from shared memory.
-// Item descriptors are loaded kStages items ahead and the queries of the next
-// item one item ahead.  Results are written in the grouped order (out[i] for
-// grouped query i).
+// in flight (cp.async) while the current one is answered from shared memory,
+// kRun queries per step.  Item descriptors are loaded kStages items ahead and
+// the queries of the next step (of this item or the next) one step ahead.
+// Results are written in the grouped order (out[i] for grouped query i).
 template <int LC>
 __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t, int f, const Item *__restrict__ items,
                                                         const int64_t *__restrict__ nitems,
@@ -213,12 +215,6 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
     stage_leaves<LC>(t, d[kStages - 1], Stage<LC>(smem + fill * stage_words, ml), ml);
     cp_async_commit();
     const Item dn = it + kStages * g < n_items ? items[it + kStages * g] : none;
-    int64_t qn[kPerThread];
-#pragma unroll
-    for (int j = 0; j < kPerThread; j++) {
-      const int r = j * kThreads + threadIdx.x;
-      qn[j] = r < d[1].len ? __ldg(qs + d[1].qa + r) : 0;
-    }
     asm volatile("cp.async.wait_group %0;" ::"n"(kStages - 1) : "memory");  // the current item's group is done
     __syncthreads();
     const Item cur = d[0];
@@ -226,26 +222,38 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
     const bool staged = cur.nl >= 1 && cur.nl <= ml;
     int span = 1;
     while (span < cur.nl) span <<= 1;
+    for (int r0 = 0; r0 < cur.len; r0 += kRun) {
+      // the next step's queries: this item's next run, else the next item's first
+      const bool more = r0 + kRun < cur.len;
+      const int32_t na = more ? cur.qa + r0 + kRun : d[1].qa;
+      const int32_t nlen = more ? cur.len - r0 - kRun : d[1].len;
+      int64_t qn[kPerThread];
 #pragma unroll
-    for (int j = 0; j < kPerThread; j++) {
-      const int r = j * kThreads + threadIdx.x;
-      if (r >= cur.len) continue;
-      int64_t v = HM_NOT_FOUND;
-      if (q[j] != kMaxKey) v = staged ? lookup_staged<LC>(st, cur.nl, span, q[j]) : lookup_scalar<LC>(t, f, q[j]);
-      out[cur.qa + r] = v;  // grouped order: consecutive threads, consecutive slots
+      for (int j = 0; j < kPerThread; j++) {
+        const int r = j * kThreads + threadIdx.x;
+        qn[j] = r < nlen ? __ldg(qs + na + r) : 0;
+      }
+#pragma unroll
+      for (int j = 0; j < kPerThread; j++) {
+        const int r = r0 + j * kThreads + threadIdx.x;
+        if (r >= cur.len) continue;
+        int64_t v = HM_NOT_FOUND;
+        if (q[j] != kMaxKey) v = staged ? lookup_staged<LC>(st, cur.nl, span, q[j]) : lookup_scalar<LC>(t, f, q[j]);
+        out[cur.qa + r] = v;  // grouped order: consecutive threads, consecutive slots
+      }
+#pragma unroll
+      for (int j = 0; j < kPerThread; j++) q[j] = qn[j];
     }
     __syncthreads();  // this stage is refilled in the next iteration
 #pragma unroll
     for (int x = 0; x < kStages - 1; x++) d[x] = d[x + 1];
     d[kStages - 1] = dn;
-#pragma unroll
-    for (int j = 0; j < kPerThread; j++) q[j] = qn[j];
     cur_stage = cur_stage == kStages - 1 ? 0 : cur_stage + 1;
   }
   cp_async_wait_all();
 }
 
-int64_t max_items(int64_t n, int nb) { return n / kRun + nb + 1; }
+int64_t max_items(int64_t n, int nb) { return n / kItemMax + nb + 1; }
 
 int leaf_bytes(int lc) { return lc == 16 ? stage_leaf_bytes<16>() : stage_leaf_bytes<64>(); }
 

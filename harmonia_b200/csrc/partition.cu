@@ -212,11 +212,18 @@ __global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_ker
 // elements sit in one contiguous run per digit (offs gives the run starts, in
 // [bucket][digit][chunk] order, so the next entry ends the run); each carries
 // its offset inside the chunk.  The results are placed by offset in shared
-// memory, then written to the chunk's input range in order.  A warp reads
-// whole runs (a lane per element, so every load is one coalesced request),
-// kRevBatch runs at a time with all their loads issued before the stores.
+// memory, then written to the chunk's input range in order.  The runs are cut
+// into units of 64 elements (a skewed batch can put most of a chunk in one
+// run); warps take units round-robin, a lane per element so every load is
+// one coalesced request, kRevBatch units at a time with all their loads
+// issued before the stores.
 constexpr int kRevWarps = kRevThreads / 32;
 constexpr int kRevBatch = HM_PSA_REV_BATCH;
+#ifndef HM_PSA_REV_UNIT
+#define HM_PSA_REV_UNIT 64  // elements of a unit of the inverse (a multiple of 32)
+#endif
+constexpr int kUnit = HM_PSA_REV_UNIT;
+constexpr int kUnitPer = kUnit / 32;
 
 __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_kernel(
     const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total, const int64_t *__restrict__ offs,
@@ -224,46 +231,71 @@ __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_ke
   extern __shared__ __align__(16) int64_t staged[];  // kChunk results
   __shared__ int64_t rs[256];
   __shared__ int32_t rl[256];
+  __shared__ int32_t up[257];  // first unit of each run
+  __shared__ uint8_t unit_run[kChunk / kUnit + 256];
+  __shared__ int32_t wsum[8];
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int len = (int)(c.end - c.begin);
-  for (int d = tid; d < nd; d += kRevThreads) {  // run of digit d: start and length
-    const int64_t k = count_index(c, d);
-    const int64_t a = offs[k];
-    rs[d] = a;
-    rl[d] = (int32_t)(offs[k + 1] - a);
+  if (tid < 256) {  // run of digit tid: start, length, units; exclusive scan of the units
+    int32_t u = 0;
+    if (tid < nd) {
+      const int64_t k = count_index(c, tid);
+      const int64_t a = offs[k];
+      const int32_t n = (int32_t)(offs[k + 1] - a);
+      rs[tid] = a;
+      rl[tid] = n;
+      u = (n + kUnit - 1) / kUnit;
+    }
+    int32_t incl = u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    up[tid] = incl - u;  // within the warp, completed below
   }
   __syncthreads();
-  for (int d0 = wid; d0 < nd; d0 += kRevWarps * kRevBatch) {
-    int64_t r[kRevBatch][2];
-    uint16_t l[kRevBatch][2];
+  if (tid < 256) {
+    int32_t add = 0;
+    for (int x = 0; x < wid; x++) add += wsum[x];
+    up[tid] += add;
+    if (tid == 255) up[256] = up[255] + (255 < nd ? (rl[255] + kUnit - 1) / kUnit : 0);
+  }
+  __syncthreads();
+  const int units = up[nd];
+  for (int d = tid; d < nd; d += kRevThreads)  // the run of every unit
+    for (int u = up[d]; u < up[d + 1]; u++) unit_run[u] = (uint8_t)d;
+  __syncthreads();
+  for (int u0 = wid; u0 < units; u0 += kRevWarps * kRevBatch) {
+    int64_t r[kRevBatch][kUnitPer];
+    uint16_t l[kRevBatch][kUnitPer];
+    int cnt[kRevBatch];
 #pragma unroll
-    for (int x = 0; x < kRevBatch; x++) {  // the first 64 elements of kRevBatch runs
-      const int d = d0 + x * kRevWarps;
-      const int n = d < nd ? rl[d] : 0;
-      const int64_t a = d < nd ? rs[d] : 0;
+    for (int x = 0; x < kRevBatch; x++) {
+      const int u = u0 + x * kRevWarps;
+      cnt[x] = 0;
+      if (u < units) {
+        const int d = unit_run[u];
+        const int e0 = (u - up[d]) * kUnit;
+        const int64_t a = rs[d] + e0;
+        cnt[x] = min(kUnit, rl[d] - e0);
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int e = lane + 32 * h;
-        if (e < n) {
-          r[x][h] = __ldg(res_in + a + e);
-          l[x][h] = __ldg(loc + a + e);
+        for (int h = 0; h < kUnitPer; h++) {
+          if (lane + 32 * h < cnt[x]) {
+            r[x][h] = __ldg(res_in + a + lane + 32 * h);
+            l[x][h] = __ldg(loc + a + lane + 32 * h);
+          }
         }
       }
     }
 #pragma unroll
-    for (int x = 0; x < kRevBatch; x++) {
-      const int d = d0 + x * kRevWarps;
-      const int n = d < nd ? rl[d] : 0;
+    for (int x = 0; x < kRevBatch; x++)
 #pragma unroll
-      for (int h = 0; h < 2; h++)
-        if (lane + 32 * h < n) staged[l[x][h]] = r[x][h];
-      if (n > 64) {  // a long run: the rest, a warp-wide step at a time
-        const int64_t a = rs[d];
-        for (int e = 64 + lane; e < n; e += 32) staged[__ldg(loc + a + e)] = __ldg(res_in + a + e);
-      }
-    }
+      for (int h = 0; h < kUnitPer; h++)
+        if (lane + 32 * h < cnt[x]) staged[l[x][h]] = r[x][h];
   }
   __syncthreads();
   for (int x = tid; x < len; x += kRevThreads) res_out[c.begin + x] = staged[x];
