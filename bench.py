@@ -203,7 +203,7 @@ def cpu_baseline_port(keys_sorted, vals_sorted, q, seconds: float = 10.0):
 def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
     """512 batches with sizes log-uniform in [1K, 4M], half uniform (90% hits),
     half Zipf(0.99) over key rank: one plain launch per batch vs the whole set
-    in one captured CUDA graph (joint pre-sort + persistent search)."""
+    in one captured CUDA graph (joint pre-sort + bucket join or search)."""
     import torch
     from harmonia_b200 import datagen as dg
 
@@ -256,8 +256,8 @@ def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
                                 "ms_per_step": round(plain_ms, 3),
                                 "what": "one search launch per batch, unsorted, group width 4, 2 queries/group"},
             "graph": {"value": round(total / plan_ms / 1e3, 1), "unit": UNIT, "ms_per_step": round(plan_ms, 3),
-                      "what": "the 512 batches in one captured CUDA graph: gather, joint 16-bit pre-sort, "
-                              "persistent search, scatter back"},
+                      "what": "the 512 batches in one captured CUDA graph: joint 16-bit pre-sort reading the "
+                              "batches in place, bucket join, inverse pre-sort writing each batch's output"},
             "speedup": round(plain_ms / plan_ms, 3)}
 
 

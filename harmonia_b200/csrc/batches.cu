@@ -9,10 +9,11 @@
 //   * small sets: one persistent search kernel whose CTAs take tiles from a
 //     global counter and find their batch by binary search over the tile
 //     prefix (no pre-sort);
-//   * large sets: the batches are gathered into one run, pre-sorted together
-//     (the query pre-sort then sees every batch at once, so even 1K-query
-//     batches share the locality of the whole set), searched, and the results
-//     scattered back to each batch's output.
+//   * large sets: the batches are pre-sorted together as one concatenation
+//     (the query pre-sort reads each batch in place and sees every batch at
+//     once, so even 1K-query batches share the locality of the whole set),
+//     searched, and the last inverse pass of the pre-sort writes each result
+//     to its batch's output.
 // Everything is enqueued on one stream with no host synchronisation and no
 // allocation, so hm_plan_create can capture it in a CUDA graph that
 // hm_plan_launch replays.
@@ -27,96 +28,60 @@ namespace hm {
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kCopyTile = 4096;
 
-// Descriptor block in device memory: batches, query prefix (nb+1), copy-tile
-// prefix (nb+1), search-tile prefix (nb+1) and the search tile counter.
+// Descriptor block in device memory: batches, query prefix (nb+1),
+// search-tile prefix (nb+1) and the search tile counter.
 struct SetLayout {
-  size_t off_batches, off_qpre, off_cpre, off_tpre, bytes;
+  size_t off_batches, off_qpre, off_tpre, bytes;
 };
 
 SetLayout set_layout(int nb) {
   SetLayout l;
   l.off_batches = 0;
   l.off_qpre = align_up((int64_t)sizeof(hm_batch) * nb, 256);
-  l.off_cpre = l.off_qpre + align_up(8 * (nb + 1), 256);
-  l.off_tpre = l.off_cpre + align_up(8 * (nb + 1), 256);
+  l.off_tpre = l.off_qpre + align_up(8 * (nb + 1), 256);
   l.bytes = l.off_tpre + align_up(8 * (nb + 2), 256);
   return l;
 }
 
-__device__ __forceinline__ int find_batch(const int64_t *__restrict__ pre, int nb, int64_t x) {
-  int lo = 0, hi = nb - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (__ldg(pre + mid) <= x) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
-// gather (dir = 0): all[qpre[b] + i] = b.q[i];  scatter back (dir = 1): b.out[i] = all[qpre[b] + i]
-__global__ void __launch_bounds__(kThreads) copy_batches_kernel(const hm_batch *__restrict__ batches,
-                                                                const int64_t *__restrict__ qpre,
-                                                                const int64_t *__restrict__ cpre, int nb,
-                                                                int64_t *__restrict__ all, int dir) {
-  const int64_t tiles = __ldg(cpre + nb);
-  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int b = find_batch(cpre, nb, tile);
-    const hm_batch bt = batches[b];
-    const int64_t i0 = (tile - __ldg(cpre + b)) * kCopyTile;
-    const int64_t i1 = min(bt.n, i0 + kCopyTile);
-    int64_t *run = all + __ldg(qpre + b);
-    if (dir == 0) {
-      for (int64_t i = i0 + threadIdx.x; i < i1; i += kThreads) run[i] = __ldg(bt.q + i);
-    } else {
-      for (int64_t i = i0 + threadIdx.x; i < i1; i += kThreads) bt.out[i] = run[i];
-    }
-  }
-}
-
 }  // namespace
 
-// Work memory of a large set: the gathered queries, the gathered results and
-// the scratch of the sorted search plan.  Small sets need none.
+// Work memory of a large set: the scratch of the sorted search plan.  Small
+// sets need none.
 size_t batches_work_bytes(const hm_tree *t, int64_t total, const SearchPlan &p) {
   if (p.bits <= 0) return 0;
-  return 2 * (size_t)align_up(total * 8, 256) + p.scratch;
+  return p.scratch;
 }
 
 // Host side: fills the descriptor block image for nb batches.
 int build_set(const hm_tree *t, const hm_batch *batches, int nb, std::vector<char> &img,
-              int64_t *total_out, int64_t *tiles_out, int64_t *copy_tiles_out) {
+              int64_t *total_out, int64_t *tiles_out) {
   const SetLayout l = set_layout(nb);
   img.assign(l.bytes, 0);
   hm_batch *b = reinterpret_cast<hm_batch *>(img.data() + l.off_batches);
   int64_t *qpre = reinterpret_cast<int64_t *>(img.data() + l.off_qpre);
-  int64_t *cpre = reinterpret_cast<int64_t *>(img.data() + l.off_cpre);
   int64_t *tpre = reinterpret_cast<int64_t *>(img.data() + l.off_tpre);
   const int tileq = search_tile_queries(t->cfg.group_width, t->cfg.queries_per_group);
-  qpre[0] = cpre[0] = tpre[0] = 0;
+  qpre[0] = tpre[0] = 0;
   for (int i = 0; i < nb; i++) {
     if (batches[i].n < 0 || (batches[i].n > 0 && (!batches[i].q || !batches[i].out))) return HM_EINVAL;
     b[i] = batches[i];
     qpre[i + 1] = qpre[i] + batches[i].n;
-    cpre[i + 1] = cpre[i] + (batches[i].n + kCopyTile - 1) / kCopyTile;
     tpre[i + 1] = tpre[i] + (batches[i].n + tileq - 1) / tileq;
   }
   tpre[nb + 1] = 0;  // tile counter, reset before every launch
   *total_out = qpre[nb];
   *tiles_out = tpre[nb];
-  *copy_tiles_out = cpre[nb];
   return HM_OK;
 }
 
 // Enqueues the whole multi-batch search on s.  d_set is the device copy of
 // the descriptor block; work has batches_work_bytes(total, plan) bytes.
-int enqueue_batches(hm_tree *t, char *d_set, int nb, int64_t total, int64_t tiles, int64_t copy_tiles,
+int enqueue_batches(hm_tree *t, char *d_set, int nb, int64_t total, int64_t tiles,
                     const SearchPlan &plan, char *work, cudaStream_t s) {
   const SetLayout l = set_layout(nb);
   const hm_batch *d_b = reinterpret_cast<const hm_batch *>(d_set + l.off_batches);
   const int64_t *qpre = reinterpret_cast<const int64_t *>(d_set + l.off_qpre);
-  const int64_t *cpre = reinterpret_cast<const int64_t *>(d_set + l.off_cpre);
   int64_t *tpre = reinterpret_cast<int64_t *>(d_set + l.off_tpre);
   if (total == 0) return HM_OK;
   if (plan.bits <= 0) {
@@ -124,17 +89,13 @@ int enqueue_batches(hm_tree *t, char *d_set, int nb, int64_t total, int64_t tile
     return launch_search_batches(t, d_b, tpre, nb, tiles, t->cfg.group_width,
                                  t->cfg.queries_per_group, s);
   }
-  const size_t a8 = align_up(total * 8, 256);
-  int64_t *all_q = reinterpret_cast<int64_t *>(work);
-  int64_t *all_out = reinterpret_cast<int64_t *>(work + a8);
-  unsigned grid = (unsigned)std::min<int64_t>(copy_tiles, (int64_t)t->num_sms * 8);
-  copy_batches_kernel<<<grid, kThreads, 0, s>>>(d_b, qpre, cpre, nb, all_q, 0);
-  note_launch();
-  int rc = run_planned_search(t, plan, all_q, total, all_out, s, work + 2 * a8);
-  if (rc) return rc;
-  copy_batches_kernel<<<grid, kThreads, 0, s>>>(d_b, qpre, cpre, nb, all_out, 1);
-  note_launch();
-  return cuda_err(cudaGetLastError());
+  // the pre-sort reads every batch's queries and the last inverse pass
+  // writes every batch's results: no gathered copy of the set
+  BatchView bv;
+  bv.batches = d_b;
+  bv.qpre = qpre;
+  bv.nb = nb;
+  return run_planned_search(t, plan, nullptr, total, nullptr, s, work, &bv);
 }
 
 }  // namespace hm
@@ -144,7 +105,7 @@ using namespace hm;
 struct hm_plan {
   hm_tree *tree = nullptr;
   int nb = 0;
-  int64_t total = 0, tiles = 0, copy_tiles = 0;
+  int64_t total = 0, tiles = 0;
   SearchPlan plan;
   char *dev = nullptr;  // descriptor block + work
   size_t dev_bytes = 0;
@@ -171,7 +132,7 @@ int capture(hm_plan *p) {
   hm_tree *t = p->tree;
   const SetLayout l = set_layout(p->nb);
   // the tile prefix depends on the search parameters: rebuild and upload it
-  int rc0 = build_set(t, p->batches.data(), p->nb, p->img, &p->total, &p->tiles, &p->copy_tiles);
+  int rc0 = build_set(t, p->batches.data(), p->nb, p->img, &p->total, &p->tiles);
   if (rc0) return rc0;
   p->plan = plan_search(t, p->total);
   const size_t need = p->img.size() + batches_work_bytes(t, p->total, p->plan);
@@ -196,7 +157,7 @@ int capture(hm_plan *p) {
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     set_capturing(true);
-    rc = enqueue_batches(t, p->dev, p->nb, p->total, p->tiles, p->copy_tiles, p->plan,
+    rc = enqueue_batches(t, p->dev, p->nb, p->total, p->tiles, p->plan,
                          p->dev + l.bytes, cs);
     set_capturing(false);
     cudaError_t e2 = cudaStreamEndCapture(cs, &p->graph);
@@ -235,8 +196,8 @@ int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream hs)
   if (nb == 0) return HM_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(hs);
   std::vector<char> img;
-  int64_t total = 0, tiles = 0, copy_tiles = 0;
-  int rc = build_set(t, batches, nb, img, &total, &tiles, &copy_tiles);
+  int64_t total = 0, tiles = 0;
+  int rc = build_set(t, batches, nb, img, &total, &tiles);
   if (rc) return rc;
   const SearchPlan plan = plan_search(t, total);
   const size_t set_bytes = img.size();
@@ -246,7 +207,7 @@ int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream hs)
   cudaError_t e = cudaMemcpyAsync(d, img.data(), set_bytes, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return cuda_err(e);
   int tok = prof_begin(t, s);
-  rc = enqueue_batches(t, d, nb, total, tiles, copy_tiles, plan, d + set_bytes, s);
+  rc = enqueue_batches(t, d, nb, total, tiles, plan, d + set_bytes, s);
   prof_end(t, kStageBatches, tok, s);
   e = cudaStreamSynchronize(s);  // img is a host buffer the copy reads
   if (rc) return rc;
@@ -262,7 +223,7 @@ int hm_plan_create(hm_tree *t, const hm_batch *batches, int nb, hm_plan **out) {
   p->tree = t;
   p->nb = nb;
   p->batches.assign(batches, batches + nb);
-  int rc = build_set(t, batches, nb, p->img, &p->total, &p->tiles, &p->copy_tiles);
+  int rc = build_set(t, batches, nb, p->img, &p->total, &p->tiles);
   if (rc) {
     delete p;
     return rc;

@@ -232,8 +232,9 @@ SearchPlan plan_search(const hm_tree *t, int64_t n) {
 }
 
 int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int64_t n, int64_t *d_out,
-                       cudaStream_t s, void *scratch) {
+                       cudaStream_t s, void *scratch, const BatchView *bv) {
   if (n <= 0) return HM_OK;
+  if (bv && p.bits <= 0) return HM_EINVAL;  // a batch set is searched through the pre-sort
   if (p.bits <= 0) {
     SearchLaunch l{d_q, d_out, nullptr, n};
     int tok = prof_begin(t, s);
@@ -247,7 +248,7 @@ int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int6
   char *ps = b + 2 * align_up(n * 8, 256);
   const int64_t *bstart = nullptr;
   int tok = prof_begin(t, s);
-  int rc = partition_queries(t, d_q, n, p.bits, qs, nullptr, ps, s, &bstart);
+  int rc = partition_queries(t, d_q, n, p.bits, qs, nullptr, ps, s, &bstart, bv);
   prof_end(t, kStagePartition, tok, s);
   if (rc) return rc;
   tok = prof_begin(t, s);
@@ -261,7 +262,7 @@ int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int6
   }
   if (rc) return rc;
   tok = prof_begin(t, s);
-  rc = unpermute_results(n, p.bits, res, d_out, ps, s);
+  rc = unpermute_results(n, p.bits, res, d_out, ps, s, bv);
   prof_end(t, kStageUnpermute, tok, s);
   return rc;
 }

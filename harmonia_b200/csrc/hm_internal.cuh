@@ -198,6 +198,14 @@ int launch_search_warm(const hm_tree *t, int group_width, int qpg);
 size_t search_smem_bytes(const hm_tree *t);
 
 // ---- query pre-sort (partition.cu) ----
+// A batch set on the device: batches[b] holds queries [qpre[b], qpre[b+1])
+// of the set's concatenation (qpre has nb + 1 entries).
+struct BatchView {
+  const hm_batch *batches = nullptr;
+  const int64_t *qpre = nullptr;
+  int nb = 0;
+};
+
 // offsets: the partition keeps chunk offsets in the scratch for
 // unpermute_results (pos_out == nullptr); else it writes input positions.
 size_t partition_scratch_bytes(int64_t n, int bits, bool offsets);
@@ -205,12 +213,15 @@ size_t partition_scratch_bytes(int64_t n, int bits, bool offsets);
 // key range); *bucket_start (if given) receives a device pointer, inside the
 // scratch, to the 2^bits + 1 bucket starts.  pos_out: original position of
 // each grouped query, or nullptr for the offset mode.
+// With bv, the queries are read from the batch set instead of q.
 int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits,
                       int64_t *q_out, int32_t *pos_out, void *scratch, cudaStream_t s,
-                      const int64_t **bucket_start = nullptr);
+                      const int64_t **bucket_start = nullptr, const BatchView *bv = nullptr);
 // Offset mode: out[i] = result of input query i, given the results in grouped
 // order (res_sorted, clobbered) and the scratch of the matching partition.
-int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, void *scratch, cudaStream_t s);
+// With bv, the results go to the batch set's outputs instead of out.
+int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, void *scratch, cudaStream_t s,
+                      const BatchView *bv = nullptr);
 
 // ---- scan, export, range (misc.cu) ----
 void scan_counts(int64_t *counts, int64_t m, cudaStream_t s);  // one-CTA in-place exclusive scan
@@ -254,7 +265,7 @@ struct SearchPlan {
 };
 SearchPlan plan_search(const hm_tree *t, int64_t n);
 int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int64_t n, int64_t *d_out,
-                       cudaStream_t s, void *scratch);
+                       cudaStream_t s, void *scratch, const BatchView *bv = nullptr);
 
 // ---- host helpers (harmonia.cu) ----
 // Point search of device-resident queries on s, with the configured pre-sort;

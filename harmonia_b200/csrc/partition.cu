@@ -87,20 +87,80 @@ __device__ __forceinline__ int64_t count_index(const Chunk &c, int d) {
   return (int64_t)c.base * 256 + (int64_t)d * c.nchunks + c.idx;
 }
 
-__global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__restrict__ q, const Chunk *__restrict__ chunks,
+// Reads and writes of a chunk [begin, end) of a flat array, or of the
+// concatenation of a batch set.  One thread resolves the chunk's batches; a
+// chunk inside one batch then goes through a single base pointer, others find
+// each element's batch among the chunk's few.
+struct ChunkIO {
+  int64_t shift;  // base = batch pointer - qpre[batch] when the chunk lies in one batch
+  int b_lo, b_hi;
+};
+
+__device__ __forceinline__ int find_batch(const int64_t *__restrict__ pre, int lo, int hi, int64_t x) {
+  while (lo < hi) {  // last b in [lo, hi] with pre[b] <= x
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(pre + mid) <= x) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  return lo;
+}
+
+template <bool BATCHED>
+__device__ __forceinline__ void resolve_chunk(const BatchView &bv, int64_t begin, int64_t end, ChunkIO *io) {
+  if constexpr (BATCHED) {
+    if (threadIdx.x == 0) {
+      io->b_lo = find_batch(bv.qpre, 0, bv.nb - 1, begin);
+      io->b_hi = find_batch(bv.qpre, io->b_lo, bv.nb - 1, end - 1);
+      io->shift = __ldg(bv.qpre + io->b_lo);
+    }
+    __syncthreads();
+  }
+}
+
+template <bool BATCHED>
+__device__ __forceinline__ int64_t read_query(const int64_t *__restrict__ q, const BatchView &bv, const ChunkIO &io,
+                                              int64_t i) {
+  if constexpr (!BATCHED) {
+    return __ldg(q + i);
+  } else {
+    const int b = io.b_lo == io.b_hi ? io.b_lo : find_batch(bv.qpre, io.b_lo, io.b_hi, i);
+    const int64_t at = b == io.b_lo ? io.shift : __ldg(bv.qpre + b);
+    return __ldg(bv.batches[b].q + (i - at));
+  }
+}
+
+template <bool BATCHED>
+__device__ __forceinline__ void write_result(int64_t *__restrict__ out, const BatchView &bv, const ChunkIO &io,
+                                             int64_t i, int64_t v) {
+  if constexpr (!BATCHED) {
+    out[i] = v;
+  } else {
+    const int b = io.b_lo == io.b_hi ? io.b_lo : find_batch(bv.qpre, io.b_lo, io.b_hi, i);
+    const int64_t at = b == io.b_lo ? io.shift : __ldg(bv.qpre + b);
+    bv.batches[b].out[i - at] = v;
+  }
+}
+
+template <bool BATCHED>
+__global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__restrict__ q, BatchView bv, const Chunk *__restrict__ chunks,
                                                         const int32_t *__restrict__ nchunks_total, Bucket bk,
                                                         int shift2, int mask2, int64_t *__restrict__ counts) {
   __shared__ unsigned hist[256];
+  __shared__ ChunkIO io;
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
   for (int i = threadIdx.x; i < 256; i += kThreads) hist[i] = 0;
+  resolve_chunk<BATCHED>(bv, c.begin, c.end, &io);
   __syncthreads();
   for (int64_t base = c.begin; base < c.end; base += 8 * kThreads) {
     int64_t k[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) {  // all loads first
       const int64_t i = base + j * kThreads + threadIdx.x;
-      k[j] = i < c.end ? __ldg(q + i) : 0;
+      k[j] = i < c.end ? read_query<BATCHED>(q, bv, io, i) : 0;
     }
 #pragma unroll
     for (int j = 0; j < 8; j++)
@@ -129,8 +189,8 @@ constexpr int stage_bytes() {
   return kTile * 16;  // one 16-B slot per staged element: key, then digit << 32 | payload
 }
 
-template <typename T, bool LOAD>
-__global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_kernel(const int64_t *__restrict__ q, const T *__restrict__ pay_in,
+template <typename T, bool LOAD, bool BATCHED>
+__global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_kernel(const int64_t *__restrict__ q, BatchView bv, const T *__restrict__ pay_in,
                                                            const Chunk *__restrict__ chunks,
                                                            const int32_t *__restrict__ nchunks_total, Bucket bk,
                                                            int shift2, int mask2, const int64_t *__restrict__ offs,
@@ -141,10 +201,12 @@ __global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_ker
   __shared__ int64_t gcur[256];
   __shared__ int64_t adj[256];
   __shared__ unsigned wsum[kThreads / 32];
+  __shared__ ChunkIO io;
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   gcur[tid] = tid <= mask2 ? offs[count_index(c, tid)] : 0;
+  resolve_chunk<BATCHED>(bv, c.begin, c.end, &io);
   int64_t k[kPer];
   T p[kPer];
   auto load_tile = [&](int64_t t0) {
@@ -152,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_ker
     for (int j = 0; j < kPer; j++) {
       const int64_t i = t0 + j * kThreads + tid;
       const bool valid = i < c.end;
-      k[j] = valid ? __ldg(q + i) : 0;
+      k[j] = valid ? read_query<BATCHED>(q, bv, io, i) : 0;
       p[j] = valid ? payload_of<T, LOAD>(pay_in, c, i) : (T)0;
     }
   };
@@ -225,19 +287,23 @@ constexpr int kRevBatch = HM_PSA_REV_BATCH;
 constexpr int kUnit = HM_PSA_REV_UNIT;
 constexpr int kUnitPer = kUnit / 32;
 
+template <bool BATCHED>
 __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_kernel(
     const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total, const int64_t *__restrict__ offs,
-    int nd, const int64_t *__restrict__ res_in, const uint16_t *__restrict__ loc, int64_t *__restrict__ res_out) {
+    int nd, const int64_t *__restrict__ res_in, const uint16_t *__restrict__ loc, int64_t *__restrict__ res_out,
+    BatchView bv) {
   extern __shared__ __align__(16) int64_t staged[];  // kChunk results
   __shared__ int64_t rs[256];
   __shared__ int32_t rl[256];
   __shared__ int32_t up[257];  // first unit of each run
   __shared__ uint8_t unit_run[kChunk / kUnit + 256];
   __shared__ int32_t wsum[8];
+  __shared__ ChunkIO io;
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int len = (int)(c.end - c.begin);
+  resolve_chunk<BATCHED>(bv, c.begin, c.end, &io);
   if (tid < 256) {  // run of digit tid: start, length, units; exclusive scan of the units
     int32_t u = 0;
     if (tid < nd) {
@@ -298,7 +364,7 @@ __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_ke
         if (lane + 32 * h < cnt[x]) staged[l[x][h]] = r[x][h];
   }
   __syncthreads();
-  for (int x = tid; x < len; x += kRevThreads) res_out[c.begin + x] = staged[x];
+  for (int x = tid; x < len; x += kRevThreads) write_result<BATCHED>(res_out, bv, io, c.begin + x, staged[x]);
 }
 
 // One CTA: chunk descriptors for a pass.  bstart == nullptr: the whole input
@@ -448,38 +514,42 @@ size_t work_layout(int64_t n, int bits, bool offsets, Work *w, char *base) {
   return off;
 }
 
-template <typename T, bool LOAD>
+template <typename T, bool LOAD, bool BATCHED = false>
 void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, const int64_t *bstart_in, int nb,
               int shift2, int mask2, int64_t *q_out, T *pay_out, int64_t *bstart_out, const Pass &ps, void *scan,
-              cudaStream_t s) {
+              cudaStream_t s, const BatchView &bv = BatchView()) {
   chunk_kernel<<<1, 1024, 0, s>>>(bstart_in, nb, n, ps.chunks, ps.nchunks);
   cudaMemsetAsync(ps.offs, 0, sizeof(int64_t) * (256 * ps.mc + 1), s);
-  psa_hist_kernel<<<(unsigned)ps.mc, kThreads, 0, s>>>(q, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs);
+  psa_hist_kernel<BATCHED><<<(unsigned)ps.mc, kThreads, 0, s>>>(q, bv, ps.chunks, ps.nchunks, bk, shift2, mask2,
+                                                                 ps.offs);
   exclusive_scan_i64(ps.offs, ps.offs, 256 * ps.mc, scan, s);
   static bool attr_set = false;  // opt in to > 48 KiB of shared memory once
   if (!attr_set) {
-    cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes<T>());
-    cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD, BATCHED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         stage_bytes<T>());
+    cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD, BATCHED>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     attr_set = true;
   }
-  psa_scatter_kernel<T, LOAD><<<(unsigned)ps.mc, kThreads, stage_bytes<T>(), s>>>(
-      q, pay_in, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs, q_out, pay_out);
+  psa_scatter_kernel<T, LOAD, BATCHED><<<(unsigned)ps.mc, kThreads, stage_bytes<T>(), s>>>(
+      q, bv, pay_in, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs, q_out, pay_out);
   const int nd = mask2 + 1;
   bucket_starts_kernel<<<(unsigned)((nb * nd + 256) / 256), 256, 0, s>>>(ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
                                                                          bstart_in, bstart_out);
   note_launch(5);
 }
 
+template <bool BATCHED = false>
 void unpermute_pass(const Pass &ps, int nd, const int64_t *res_in, const uint16_t *loc, int64_t *res_out,
-                    cudaStream_t s) {
+                    cudaStream_t s, const BatchView &bv = BatchView()) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(psa_unpermute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(8 * kChunk));
-    cudaFuncSetAttribute(psa_unpermute_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(psa_unpermute_kernel<BATCHED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(8 * kChunk));
+    cudaFuncSetAttribute(psa_unpermute_kernel<BATCHED>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     attr_set = true;
   }
-  psa_unpermute_kernel<<<(unsigned)ps.mc, kRevThreads, 8 * kChunk, s>>>(ps.chunks, ps.nchunks, ps.offs, nd, res_in,
-                                                                        loc, res_out);
+  psa_unpermute_kernel<BATCHED><<<(unsigned)ps.mc, kRevThreads, 8 * kChunk, s>>>(ps.chunks, ps.nchunks, ps.offs, nd,
+                                                                                 res_in, loc, res_out, bv);
   note_launch();
 }
 
@@ -490,15 +560,19 @@ size_t partition_scratch_bytes(int64_t n, int bits, bool offsets) {
 }
 
 int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, int64_t *q_out, int32_t *pos_out,
-                      void *scratch, cudaStream_t s, const int64_t **bucket_start) {
+                      void *scratch, cudaStream_t s, const int64_t **bucket_start, const BatchView *bv) {
   if (n == 0) return HM_OK;
   if (bits < 1 || bits > 16 || n > INT32_MAX || n < 0) return HM_EINVAL;
   const bool offsets = pos_out == nullptr;
+  if (bv && !offsets) return HM_EINVAL;
   Work w;
   work_layout(n, bits, offsets, &w, static_cast<char *>(scratch));
   const Bucket bk = make_bucket(t, bits);
   if (bits <= 8) {
-    if (offsets)
+    if (bv)
+      one_pass<uint16_t, false, true>(bk, nullptr, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, w.loc,
+                                      w.bstart, w.p1, w.scan, s, *bv);
+    else if (offsets)
       one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, w.loc, w.bstart, w.p1,
                                 w.scan, s);
     else
@@ -508,7 +582,12 @@ int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, i
     const int low = bits - 8;
     if (offsets) {
       uint16_t *loc1 = static_cast<uint16_t *>(w.pay1);
-      one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1, w.p1, w.scan, s);
+      if (bv)
+        one_pass<uint16_t, false, true>(bk, nullptr, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1,
+                                        w.p1, w.scan, s, *bv);
+      else
+        one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1, w.p1, w.scan,
+                                  s);
       one_pass<uint16_t, false>(bk, w.q_tmp, nullptr, n, w.bstart1, 256, 0, (1 << low) - 1, q_out, w.loc, w.bstart,
                                 w.p2, w.scan, s);
     } else {
@@ -522,17 +601,24 @@ int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, i
   return cuda_err(cudaGetLastError());
 }
 
-int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, void *scratch, cudaStream_t s) {
+int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, void *scratch, cudaStream_t s,
+                      const BatchView *bv) {
   if (n == 0) return HM_OK;
   if (bits < 1 || bits > 16 || n > INT32_MAX || n < 0) return HM_EINVAL;
   Work w;
   work_layout(n, bits, true, &w, static_cast<char *>(scratch));
-  if (bits <= 8) {
-    unpermute_pass(w.p1, 1 << bits, res_sorted, w.loc, out, s);
-  } else {
+  const int64_t *res1 = res_sorted;  // results in first-pass order
+  const uint16_t *loc1 = w.loc;
+  if (bits > 8) {
     unpermute_pass(w.p2, 1 << (bits - 8), res_sorted, w.loc, w.q_tmp, s);
-    unpermute_pass(w.p1, 256, w.q_tmp, static_cast<const uint16_t *>(w.pay1), out, s);
+    res1 = w.q_tmp;
+    loc1 = static_cast<const uint16_t *>(w.pay1);
   }
+  const int nd1 = bits <= 8 ? 1 << bits : 256;
+  if (bv)
+    unpermute_pass<true>(w.p1, nd1, res1, loc1, nullptr, s, *bv);
+  else
+    unpermute_pass(w.p1, nd1, res1, loc1, out, s);
   return cuda_err(cudaGetLastError());
 }
 
