@@ -535,7 +535,7 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
   const int nd = mask2 + 1;
   bucket_starts_kernel<<<(unsigned)((nb * nd + 256) / 256), 256, 0, s>>>(ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
                                                                          bstart_in, bstart_out);
-  note_launch(5);
+  note_launch(4);  // chunk, histogram, scatter, bucket starts (the scan counts its own)
 }
 
 template <bool BATCHED = false>
