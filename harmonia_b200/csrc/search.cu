@@ -26,6 +26,7 @@
 //     (the reference returns a (leaf, slot) pair decoded on the host,
 //     open-harmonia/src/full-multi-prefix-sort-8thread.cu:34-39,454-476).
 #include "hm_internal.cuh"
+#include "async_copy.cuh"
 
 #include <cstdio>
 
@@ -34,7 +35,6 @@ namespace hm {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr long kSpinLimit = 1l << 24;
 
 struct Args {
   DevTree t;
@@ -50,51 +50,6 @@ struct Args {
   unsigned long long *tile_counter;
   unsigned *err;
 };
-
-__device__ __forceinline__ unsigned smem_addr(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, "
-      "0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for phase 0 of bar; false if the limit was reached.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar) {
-  for (long i = 0; i < kSpinLimit; i++)
-    if (mbar_try_wait(bar, 0)) return true;
-  return false;
-}
 
 // L2 cache policies (createpolicy): inner rows are re-read by every query and
 // should stay in L2; leaf rows are touched about once per batch.
