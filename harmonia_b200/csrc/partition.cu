@@ -40,14 +40,18 @@ constexpr int kThreads = 256;
 #define HM_PSA_TILE 4096  // queries a scatter CTA stages at a time
 #endif
 constexpr int kTile = HM_PSA_TILE;
-constexpr int kPer = kTile / kThreads;
-static_assert(kTile % kThreads == 0 && kTile <= 65536, "ranks are kept in 16 bits");
 constexpr int64_t kChunk = 8192;  // queries per CTA chunk (a multiple of kTile; offsets fit 16 bits)
 
 // Launch shapes (compile-time tunables, measured on B200 at 2^24 queries).
+#ifndef HM_PSA_SCATTER_THREADS
+#define HM_PSA_SCATTER_THREADS 256  // threads of a scatter CTA (256, 512 or 1024)
+#endif
 #ifndef HM_PSA_SCATTER_MINB
 #define HM_PSA_SCATTER_MINB 3  // resident scatter CTAs per SM the register budget allows
 #endif
+constexpr int kSc = HM_PSA_SCATTER_THREADS;
+constexpr int kPer = kTile / kSc;
+static_assert(kSc >= 256 && kTile % kSc == 0 && kTile <= 65536, "a thread per digit; ranks kept in 16 bits");
 #ifndef HM_PSA_REV_THREADS
 #define HM_PSA_REV_THREADS 512
 #endif
@@ -190,7 +194,7 @@ constexpr int stage_bytes() {
 }
 
 template <typename T, bool LOAD, bool BATCHED>
-__global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_kernel(const int64_t *__restrict__ q, BatchView bv, const T *__restrict__ pay_in,
+__global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(const int64_t *__restrict__ q, BatchView bv, const T *__restrict__ pay_in,
                                                            const Chunk *__restrict__ chunks,
                                                            const int32_t *__restrict__ nchunks_total, Bucket bk,
                                                            int shift2, int mask2, const int64_t *__restrict__ offs,
@@ -200,19 +204,20 @@ __global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_ker
   __shared__ unsigned tstart[256];
   __shared__ int64_t gcur[256];
   __shared__ int64_t adj[256];
-  __shared__ unsigned wsum[kThreads / 32];
+  __shared__ unsigned wsum[8];
   __shared__ ChunkIO io;
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  gcur[tid] = tid <= mask2 ? offs[count_index(c, tid)] : 0;
+  const bool digit_thread = tid < 256;  // threads 0..255 own a digit's counters
+  if (digit_thread) gcur[tid] = tid <= mask2 ? offs[count_index(c, tid)] : 0;
   resolve_chunk<BATCHED>(bv, c.begin, c.end, &io);
   int64_t k[kPer];
   T p[kPer];
   auto load_tile = [&](int64_t t0) {
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
-      const int64_t i = t0 + j * kThreads + tid;
+      const int64_t i = t0 + j * kSc + tid;
       const bool valid = i < c.end;
       k[j] = valid ? read_query<BATCHED>(q, bv, io, i) : 0;
       p[j] = valid ? payload_of<T, LOAD>(pay_in, c, i) : (T)0;
@@ -220,12 +225,12 @@ __global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_ker
   };
   load_tile(c.begin);
   for (int64_t t0 = c.begin; t0 < c.end; t0 += kTile) {
-    cnt[tid] = 0;
+    if (digit_thread) cnt[tid] = 0;
     __syncthreads();
     unsigned dr[kPer];  // digit << 16 | rank inside the tile's digit run; ~0u past the end
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
-      if (t0 + j * kThreads + tid < c.end) {
+      if (t0 + j * kSc + tid < c.end) {
         const unsigned d = (unsigned)((bk(k[j]) >> shift2) & mask2);
         dr[j] = d << 16 | atomicAdd(&cnt[d], 1u);
       } else {
@@ -233,20 +238,25 @@ __global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_ker
       }
     }
     __syncthreads();
-    // exclusive scan of the 256 tile counts (one per thread)
-    const unsigned mine = cnt[tid];
-    unsigned incl = mine;
+    // exclusive scan of the 256 tile counts (one per digit thread)
+    unsigned mine = 0, incl = 0;
+    if (digit_thread) {
+      mine = cnt[tid];
+      incl = mine;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) wsum[w] = incl;
     }
-    if (lane == 31) wsum[w] = incl;
     __syncthreads();
-    unsigned before = incl - mine;
-    for (int x = 0; x < w; x++) before += wsum[x];
-    tstart[tid] = before;
-    adj[tid] = gcur[tid] - (int64_t)before;  // slot sl of digit d goes to adj[d] + sl
+    if (digit_thread) {
+      unsigned before = incl - mine;
+      for (int x = 0; x < w; x++) before += wsum[x];
+      tstart[tid] = before;
+      adj[tid] = gcur[tid] - (int64_t)before;  // slot sl of digit d goes to adj[d] + sl
+    }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
@@ -259,14 +269,14 @@ __global__ void __launch_bounds__(kThreads, HM_PSA_SCATTER_MINB) psa_scatter_ker
     __syncthreads();
     if (t0 + kTile < c.end) load_tile(t0 + kTile);  // the next tile's loads overlap the write-out
     const int n = (int)min((int64_t)kTile, c.end - t0);
-    for (int sl = tid; sl < n; sl += kThreads) {
+    for (int sl = tid; sl < n; sl += kSc) {
       const longlong2 e = slot[sl];
       const int64_t o = adj[(uint64_t)e.y >> 32] + sl;
       q_out[o] = e.x;
       pay_out[o] = (T)(uint32_t)e.y;
     }
     __syncthreads();
-    gcur[tid] += cnt[tid];
+    if (digit_thread) gcur[tid] += cnt[tid];
   }
 }
 
@@ -530,7 +540,7 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
     cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD, BATCHED>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     attr_set = true;
   }
-  psa_scatter_kernel<T, LOAD, BATCHED><<<(unsigned)ps.mc, kThreads, stage_bytes<T>(), s>>>(
+  psa_scatter_kernel<T, LOAD, BATCHED><<<(unsigned)ps.mc, kSc, stage_bytes<T>(), s>>>(
       q, bv, pay_in, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs, q_out, pay_out);
   const int nd = mask2 + 1;
   bucket_starts_kernel<<<(unsigned)((nb * nd + 256) / 256), 256, 0, s>>>(ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
