@@ -72,8 +72,8 @@ typedef struct {
   int cache_hints;       /* L2 policy: 1 = inner rows evict_last, leaves evict_first; 2 = none
                             (default 1) */
   int join;              /* large batches: 1 = pre-sort + bucket join, 2 = never, -1 = when the
-                            batch has at least half as many queries as the tree has leaves
-                            and 2^20 queries (default -1) */
+                            batch has at least 4 queries per leaf and 2^22 queries, or at least
+                            the sample size at which hm_autotune saw the join win (default -1) */
 } hm_config;
 
 /* Read-only description of a loaded tree. */
