@@ -261,6 +261,44 @@ def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
             "speedup": round(plain_ms / plan_ms, 3)}
 
 
+def fanout_128(keys, q, d_q, dev, timed, steps, warmup, exp):
+    """The same keys and batch on a fanout-128 tree: the descent unsorted, the
+    descent on a batch pre-sorted by its top 16 key bits, and the tuned path.
+    Algorithmic bytes of the descent at fanout 128: 240 B per query (the last
+    inner level, 1 KiB rows, is no longer L2-resident)."""
+    import torch
+    from harmonia_b200 import BPlusTree, datagen as dg
+
+    m = len(q)
+    t = BPlusTree.bulk_load(torch.from_numpy(keys).to(dev), torch.from_numpy(dg.values_for(keys)).to(dev),
+                            fanout=128)
+    out = torch.empty_like(d_q)
+    res = {"tree": {"height": int(t.info().height), "n_leaf": int(t.info().n_leaf)}}
+
+    def run(name, qq, what, bq=None):
+        for _ in range(warmup):
+            t.search(qq, out)
+        ms = timed(steps, lambda: t.search(qq, out))
+        r = {"value": round(m / ms / 1e3, 1), "unit": UNIT, "ms_per_step": round(ms, 4), "what": what}
+        if bq:
+            r["algorithmic_gbs"] = round(bq * m / (ms * 1e-3) / 1e9, 1)
+        res[name] = r
+
+    t.set_search_config(group_width=4, queries_per_group=2, sort_bits=0, join=2)
+    run("plain", d_q, "one descent launch on the unsorted batch, group width 4, 2 queries per group", 240)
+    assert (out[:4096].cpu().numpy() == exp).all(), "fanout-128 results are wrong"
+    order = np.argsort(q >> np.int64(47), kind="stable")
+    d_qs = torch.from_numpy(q[order]).to(dev)
+    run("presorted_input", d_qs, "the same launch on the batch pre-sorted by its top 16 key bits", 240)
+    del d_qs
+    tuned = t.autotune(d_q)
+    run("tuned", d_q, "the autotuned path (descent settings, and the bucket join where it wins)")
+    assert (out[:4096].cpu().numpy() == exp).all(), "fanout-128 results are wrong"
+    res["tuned"]["config"] = {k: tuned[k] for k in ("group_width", "queries_per_group", "sort_bits", "join")}
+    t.close()
+    return res
+
+
 def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
     """Serving workload: a 2^25-key tree; Poisson arrivals, request sizes
     log-uniform in [64, 2^20]; 90% point search (80% hits), 5% range (length
@@ -477,6 +515,8 @@ def main():
     if args.extras:
         extras["batched_uneven"] = batched_uneven(tree, keys, sk, dev, timed, max(3, args.steps // 3),
                                                   args.warmup)
+    if args.extras and args.fanout == 64:
+        extras["fanout_128"] = fanout_128(keys, q, d_q, dev, timed, args.steps, args.warmup, exp)
 
     # ---- end to end through the public API with host (pinned) buffers ----
     h_q = torch.from_numpy(q).pin_memory()

@@ -300,6 +300,7 @@ const char *hm_strerror(int code) {
     case HM_EBUSY: return "busy: queue full or memory budget exhausted";
     case HM_ECANCELLED: return "request cancelled or server stopped";
     case HM_ETOOLARGE: return "size exceeds a documented maximum";
+    case HM_EIO: return "file missing, unreadable, unwritable or malformed";
     default: return "unknown error";
   }
 }

@@ -15,7 +15,7 @@ HM_OK = 0
 ERRORS = {
     -1: "HM_EINVAL", -2: "HM_ENOMEM", -3: "HM_EDUPLICATE", -4: "HM_EMAXKEY", -5: "HM_ECUDA",
     -6: "HM_ECAPACITY", -7: "HM_ETIMEOUT", -8: "HM_ENODEVICE", -9: "HM_EBUSY",
-    -10: "HM_ECANCELLED", -11: "HM_ETOOLARGE",
+    -10: "HM_ECANCELLED", -11: "HM_ETOOLARGE", -12: "HM_EIO",
 }
 HM_UPSERT_SUPPLIED = 0
 HM_UPSERT_REF_KEY_MINUS_1 = 1
@@ -28,7 +28,8 @@ EXPORTS = (
     "hm_profile", "hm_profile_read", "hm_plan_create", "hm_plan_launch", "hm_plan_free",
     "hm_search_noalloc", "hm_server_config_default", "hm_server_start", "hm_server_submit",
     "hm_server_wait", "hm_server_get_stats", "hm_server_reset_stats", "hm_server_stop", "hm_server_free",
-    "hm_last_cuda_error",
+    "hm_last_cuda_error", "hm_read_keys", "hm_read_ranges", "hm_write_keys", "hm_snapshot_save",
+    "hm_snapshot_load",
 )
 HM_NOALLOC_MAX_QUERIES = 1 << 20
 
@@ -113,6 +114,12 @@ def lib() -> ctypes.CDLL:
     L.hm_plan_free.argtypes = [P]
     L.hm_search_noalloc.argtypes = [P, P, SZ, P, P]
     L.hm_profile_read.argtypes = [P, ctypes.POINTER(StageTime), I, ctypes.POINTER(I)]
+    C = ctypes.c_char_p
+    L.hm_read_keys.argtypes = [C, P, SZ, ctypes.POINTER(SZ)]
+    L.hm_read_ranges.argtypes = [C, P, P, SZ, ctypes.POINTER(SZ)]
+    L.hm_write_keys.argtypes = [C, P, SZ]
+    L.hm_snapshot_save.argtypes = [P, C]
+    L.hm_snapshot_load.argtypes = [C, ctypes.POINTER(Config), PT]
     _lib = L
     return L
 

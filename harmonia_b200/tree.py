@@ -23,6 +23,7 @@ come back in the same kind.  Errors raise HarmoniaError with the HM_E* code.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -99,6 +100,32 @@ class BPlusTree:
         n = len(keys)
         check(lib().hm_bulk_load(_ptr(keys) if n else None, _ptr(values) if n else None, n,
                                  ctypes.byref(cfg), ctypes.byref(h)), "hm_bulk_load")
+        return cls(h.value)
+
+    @classmethod
+    def from_reference_file(cls, path: str, **config) -> "BPlusTree":
+        """Bulk-loads the keys of a reference insert file (one decimal key per
+        line) with value = key, as the reference's main() inserts them
+        (open-harmonia/src/main.cpp:56-66)."""
+        from .files import read_keys
+
+        keys = read_keys(path)
+        return cls.bulk_load(keys, keys.copy(), **config)
+
+    def save(self, path: str) -> None:
+        """Writes a snapshot (sorted contents + configuration) to path."""
+        check(lib().hm_snapshot_save(self._h, os.fsencode(path)), "hm_snapshot_save")
+
+    @classmethod
+    def load(cls, path: str, **config) -> "BPlusTree":
+        """Bulk-loads a snapshot; keyword arguments override the saved
+        configuration (fanout, leaf_cap, fills, search settings)."""
+        h = ctypes.c_void_p()
+        cfg = None
+        if config:
+            cfg = native.default_config(**config)
+        check(lib().hm_snapshot_load(os.fsencode(path), ctypes.byref(cfg) if cfg is not None else None,
+                                     ctypes.byref(h)), "hm_snapshot_load")
         return cls(h.value)
 
     def close(self) -> None:

@@ -49,7 +49,8 @@ enum {
   HM_ENODEVICE = -8,   /* no usable CUDA device */
   HM_EBUSY = -9,       /* serving: queue full or budget exhausted */
   HM_ECANCELLED = -10, /* serving: request cancelled or server stopped */
-  HM_ETOOLARGE = -11   /* a size exceeds a documented maximum */
+  HM_ETOOLARGE = -11,  /* a size exceeds a documented maximum */
+  HM_EIO = -12         /* a file could not be opened, read or written, or is malformed */
 };
 
 typedef void *hm_stream; /* a cudaStream_t; NULL = the legacy default stream */
@@ -293,9 +294,37 @@ int hm_profile(hm_tree *t, int enable);
  * sets *n, and clears the record. */
 int hm_profile_read(hm_tree *t, hm_stage_time *out, int cap, int *n);
 
+/* ---- Reference dataset files and tree snapshots ------------------------- */
+
+/* Reads a key file in the reference's text format: one signed decimal key per
+ * line, as open-harmonia/script/generate-data/generate.py writes insert,
+ * search and update files and open-harmonia/src/main.cpp:50-67 reads them
+ * (sscanf "%lld": leading blanks skipped, text after the number ignored).
+ * Call with keys == NULL to get the count in *n, then again with cap >= *n.
+ * Blank lines are skipped; a line without a number gives HM_EIO. */
+int hm_read_keys(const char *path, int64_t *keys, size_t cap, size_t *n);
+
+/* Reads a range file in the reference's format: two lines per query, the
+ * start key then the end key (open-harmonia/src/range.cu:349-355 reads the
+ * pairs; its GPU path then ignores the end).  Count as hm_read_keys. */
+int hm_read_ranges(const char *path, int64_t *start, int64_t *end, size_t cap, size_t *n);
+
+/* Writes keys in the same text format, one per line. */
+int hm_write_keys(const char *path, const int64_t *keys, size_t n);
+
+/* Writes the tree's contents (keys in order with their values) and its
+ * configuration to a binary file, with a checksum.  No counterpart in the
+ * reference, whose trees live only in process memory. */
+int hm_snapshot_save(hm_tree *t, const char *path);
+
+/* Bulk-loads a tree from a snapshot; cfg == NULL uses the saved
+ * configuration.  HM_EIO for a missing, truncated or corrupted file. */
+int hm_snapshot_load(const char *path, const hm_config *cfg, hm_tree **out);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
+
 #ifdef __cplusplus
 }
 #endif
