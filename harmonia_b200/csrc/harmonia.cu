@@ -53,7 +53,7 @@ int ensure_scratch(hm_tree *t, size_t bytes) {
 }
 
 static const char *kStageNames[kStageCount] = {"partition", "search", "search_batches", "range",
-                                               "upsert", "join", "unpermute"};
+                                               "upsert", "join", "unpermute", "delete"};
 
 static cudaEvent_t prof_event(hm_tree *t) {
   if (!t->prof_pool.empty()) {
@@ -688,6 +688,36 @@ int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n_, in
     rc = cuda_err(e);
   }
   cudaFree(tk);
+  return rc ? rc : hm_sync(t, hs);
+}
+
+int hm_delete_batch(hm_tree *t, const int64_t *keys, size_t n_, size_t *removed, hm_stream hs) {
+  if (removed) *removed = 0;
+  if (!t || (n_ > 0 && !keys)) return HM_EINVAL;
+  const int64_t n = (int64_t)n_;
+  if (n == 0) return HM_OK;
+  cudaStream_t s = as_stream(hs);
+  const int64_t *dk = keys;
+  int64_t *tmp = nullptr;
+  if (!is_device_ptr(keys)) {
+    cudaError_t e = cudaMalloc(&tmp, (size_t)align_up(n * 8, 256));
+    if (e != cudaSuccess) return cuda_err(e);
+    e = cudaMemcpyAsync(tmp, keys, n * 8, cudaMemcpyDefault, s);
+    if (e != cudaSuccess) {
+      cudaFree(tmp);
+      return cuda_err(e);
+    }
+    dk = tmp;
+  }
+  int64_t gone = 0;
+  int tok = prof_begin(t, s);
+  int rc = delete_epoch(t, dk, n, &gone, s);
+  prof_end(t, kStageDelete, tok, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (tmp) cudaFree(tmp);
+  if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
+  if (removed) *removed = (size_t)gone;
+  choose_smem_levels(t);
   return rc ? rc : hm_sync(t, hs);
 }
 

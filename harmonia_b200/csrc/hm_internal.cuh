@@ -237,12 +237,14 @@ int range_copy_out(const hm_tree *t, const int32_t *first_leaf, const int32_t *f
                    const int64_t *offsets, int64_t n, int64_t *okeys, int64_t *ovals, cudaStream_t s);
 
 // ---- upsert (upsert.cu) ----
+int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed, cudaStream_t s);
+int rebuild_from_sorted(hm_tree *t, const uint64_t *ck, const int64_t *cv, int64_t n1, cudaStream_t s);
 int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64_t n,
                  int flags, cudaStream_t s);
 
 // ---- stage timing ----
 enum Stage { kStagePartition = 0, kStageSearch, kStageBatches, kStageRange, kStageUpsert, kStageJoin,
-             kStageUnpermute, kStageCount };
+             kStageUnpermute, kStageDelete, kStageCount };
 // Records the start event of a stage on stream s (no-op unless profiling).
 int prof_begin(hm_tree *t, cudaStream_t s);
 void prof_end(hm_tree *t, int stage, int token, cudaStream_t s);

@@ -66,6 +66,7 @@ struct Slot {
 size_t req_device_bytes(const hm_request &r) {
   switch (r.kind) {
     case HM_REQ_SEARCH: return 16 * r.n;
+    case HM_REQ_DELETE: return 8 * r.n;
     case HM_REQ_RANGE: {
       size_t recs = 0;
       for (size_t i = 0; i < r.n; i++) recs += r.lens[i] > 0 ? (size_t)r.lens[i] : 0;
@@ -312,6 +313,7 @@ void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
     return;
   }
   Slot &sl = *fs;
+  const bool del = ups[0]->r.kind == HM_REQ_DELETE;
   const size_t b = align_up(std::max<int64_t>(n, 1) * 8, 256);
   int rc = slot_reserve(sl, 2 * b, 2 * b);
   if (rc == HM_OK && n > 0) {
@@ -320,15 +322,16 @@ void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
     int64_t o = 0;
     for (Req *q : ups) {
       std::memcpy(hk + o, q->r.keys, q->r.n * 8);
-      std::memcpy(hv + o, q->r.vals, q->r.n * 8);
+      if (!del) std::memcpy(hv + o, q->r.vals, q->r.n * 8);
       o += (int64_t)q->r.n;
     }
     int64_t *dk = reinterpret_cast<int64_t *>(sl.dev);
     int64_t *dv = reinterpret_cast<int64_t *>(sl.dev + b);
     cudaError_t e = cudaMemcpyAsync(dk, hk, n * 8, cudaMemcpyHostToDevice, sl.s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dv, hv, n * 8, cudaMemcpyHostToDevice, sl.s);
+    if (e == cudaSuccess && !del) e = cudaMemcpyAsync(dv, hv, n * 8, cudaMemcpyHostToDevice, sl.s);
     rc = cuda_err(e);
-    if (rc == HM_OK) rc = upsert_epoch(t, dk, dv, n, ups[0]->r.flags, sl.s);
+    if (rc == HM_OK)
+      rc = del ? delete_epoch(t, dk, n, nullptr, sl.s) : upsert_epoch(t, dk, dv, n, ups[0]->r.flags, sl.s);
     e = cudaStreamSynchronize(sl.s);
     if (rc == HM_OK) rc = cuda_err(e);
     refresh_smem_levels(t);
@@ -356,10 +359,12 @@ void dispatcher(hm_server *sv) {
       }
       Req *head = sv->queue.front();
       kind = head->r.kind;
-      if (kind == HM_REQ_UPSERT) {
-        while (!sv->queue.empty() && sv->queue.front()->r.kind == HM_REQ_UPSERT) {
+      if (kind == HM_REQ_UPSERT || kind == HM_REQ_DELETE) {
+        // one epoch: consecutive writes of the head's kind (upserts of one rule)
+        while (!sv->queue.empty() && sv->queue.front()->r.kind == kind) {
           Req *q = sv->queue.front();
-          if (!take.empty() && (q->r.flags != HM_UPSERT_SUPPLIED || take[0]->r.flags != HM_UPSERT_SUPPLIED))
+          if (kind == HM_REQ_UPSERT && !take.empty() &&
+              (q->r.flags != HM_UPSERT_SUPPLIED || take[0]->r.flags != HM_UPSERT_SUPPLIED))
             break;
           take.push_back(q);
           sv->queue.pop_front();
@@ -404,7 +409,7 @@ void dispatcher(hm_server *sv) {
         free_slot->reqs = take;
       }
     }
-    if (kind == HM_REQ_UPSERT) {
+    if (kind == HM_REQ_UPSERT || kind == HM_REQ_DELETE) {
       run_epoch(sv, take);
       continue;
     }
@@ -451,6 +456,9 @@ int check_request(const hm_request *r) {
     case HM_REQ_UPSERT:
       if (r->n > 0 && (!r->keys || !r->vals)) return HM_EINVAL;
       if (r->flags != HM_UPSERT_SUPPLIED && r->flags != HM_UPSERT_REF_KEY_MINUS_1) return HM_EINVAL;
+      return HM_OK;
+    case HM_REQ_DELETE:
+      if (r->n > 0 && !r->keys) return HM_EINVAL;
       return HM_OK;
     default:
       return HM_EINVAL;

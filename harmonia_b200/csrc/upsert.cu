@@ -207,9 +207,125 @@ __global__ void merge_rank_kernel(const int64_t *__restrict__ a, const int64_t *
   }
 }
 
+// ---- delete epochs ----
+
+__global__ void compact_keys_kernel(const uint64_t *__restrict__ uk, const int32_t *__restrict__ keep,
+                                    const int64_t *__restrict__ at, int64_t n, int64_t *__restrict__ bk) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (keep[i]) bk[at[i]] = (int64_t)(uk[i] ^ kSign);
+}
+
+// One thread per distinct key: descend; a stored key's slot is overwritten
+// with Max_Key (the leaf is compacted next); route[i] = the key's leaf.
+__global__ void delete_mark_kernel(DevTree t, int f, int lc, int li, const int64_t *__restrict__ bk, int64_t m,
+                                   int64_t *leaf_rows, int32_t *__restrict__ route) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = bk[i];
+    const int32_t leaf = descend_leaf(t, f, k == kMaxKey ? kMaxKey - 1 : k);  // never rank the sentinel
+    route[i] = leaf;
+    if (k == kMaxKey) continue;  // never stored
+    int64_t *kr = leaf_rows + (int64_t)leaf * (li + 2 * lc) + li;
+    const int cnt = t.leaf_cnt[leaf];
+    for (int s = 0; s < cnt; s++)
+      if (kr[s] == k) kr[s] = kMaxKey;
+  }
+}
+
+// One thread per leaf the batch routed to (keys are sorted, so each leaf's
+// keys are one run of route[]): squeeze out the marked slots keeping key
+// order, refresh the leaf index words, count what went; flags bit0 when a
+// leaf that held keys is left empty (the tree is then rebuilt).
+__global__ void delete_compact_kernel(int64_t *leaf_rows, int32_t *leaf_cnt, int lc, int li,
+                                      const int32_t *__restrict__ route, int64_t m,
+                                      unsigned long long *removed, unsigned *flags) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i > 0 && route[i - 1] == route[i]) continue;
+    const int32_t leaf = route[i];
+    int64_t *row = leaf_rows + (int64_t)leaf * (li + 2 * lc);
+    int64_t *kr = row + li, *vr = kr + lc;
+    const int cnt = leaf_cnt[leaf];
+    int live = 0;
+    for (int s = 0; s < cnt; s++) {
+      if (kr[s] == kMaxKey) continue;
+      kr[live] = kr[s];
+      vr[live] = vr[s];
+      live++;
+    }
+    if (live == cnt) continue;
+    for (int s = live; s < cnt; s++) {
+      kr[s] = kMaxKey;
+      vr[s] = HM_NOT_FOUND;
+    }
+    for (int x = 0; x < li; x++) row[x] = (8 * (x + 1) < lc) ? kr[8 * (x + 1)] : kMaxKey;
+    leaf_cnt[leaf] = live;
+    atomicAdd(removed, (unsigned long long)(cnt - live));
+    if (live == 0) atomicOr(flags, 1u);
+  }
+}
+
 size_t al(int64_t bytes) { return (size_t)align_up(bytes, 256); }
 
 }  // namespace
+
+// Bulk-loads n1 sorted (sign-flipped) keys and their values into a fresh arena
+// with the tree's parameters and swaps it in; the old arena is freed.
+int rebuild_from_sorted(hm_tree *t, const uint64_t *ck, const int64_t *cv, int64_t n1, cudaStream_t s) {
+  hm_tree nt = *t;  // new shape in a copy; arena swapped in at the end
+  nt.scratch = nullptr;
+  int rc = shape(n1, t->cfg, &nt.height, nt.lvl_start, &nt.n_inner, &nt.n_leaf);
+  if (rc) return rc;
+  size_t off_prefix = al(nt.n_inner * nt.inner_row * 8);
+  size_t off_lrows = off_prefix + al(align_up(nt.n_inner, 4) * 4);
+  size_t off_lcnt = off_lrows + al(nt.n_leaf * nt.leaf_row * 8);
+  size_t off_lbase = off_lcnt + al(nt.n_leaf * 4);
+  size_t total = off_lbase + al(nt.n_leaf * 8);
+  int64_t tn = std::max<int64_t>(std::max<int64_t>(n1, nt.n_leaf), 1);
+  char *tmp = nullptr;
+  cudaError_t e = cudaMalloc(&nt.arena, total);
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, 2 * al(8 * tn));
+  if (e != cudaSuccess) {
+    if (nt.arena) cudaFree(nt.arena);
+    if (tmp) cudaFree(tmp);
+    return cuda_err(e);
+  }
+  int64_t *tmp_a = reinterpret_cast<int64_t *>(tmp);
+  int64_t *tmp_b = reinterpret_cast<int64_t *>(tmp + al(8 * tn));
+  char *base = static_cast<char *>(nt.arena);
+  cudaMemsetAsync(base, 0, total, s);
+  nt.arena_bytes = total;
+  nt.inner = reinterpret_cast<int64_t *>(base);
+  nt.prefix = reinterpret_cast<int32_t *>(base + off_prefix);
+  nt.leaf_rows = reinterpret_cast<int64_t *>(base + off_lrows);
+  nt.leaf_cnt = reinterpret_cast<int32_t *>(base + off_lcnt);
+  nt.leaf_base = reinterpret_cast<int64_t *>(base + off_lbase);
+  nt.n_keys = n1;
+  rc = build_from_sorted(&nt, ck, cv, n1, tmp_a, tmp_b, s);
+  e = cudaStreamSynchronize(s);
+  cudaFree(tmp);
+  if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
+  if (rc) {
+    cudaFree(nt.arena);
+    return rc;
+  }
+  cudaFree(t->arena);
+  t->arena = nt.arena;
+  t->arena_bytes = nt.arena_bytes;
+  t->inner = nt.inner;
+  t->prefix = nt.prefix;
+  t->leaf_rows = nt.leaf_rows;
+  t->leaf_cnt = nt.leaf_cnt;
+  t->leaf_base = nt.leaf_base;
+  t->height = nt.height;
+  std::memcpy(t->lvl_start, nt.lvl_start, sizeof(t->lvl_start));
+  t->n_inner = nt.n_inner;
+  t->n_leaf = nt.n_leaf;
+  t->n_keys = n1;
+  t->generation++;
+  return HM_OK;
+}
 
 int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64_t n, int flags,
                  cudaStream_t s) {
@@ -314,72 +430,113 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     // Rebuild: contents (already carrying this epoch's in-place updates)
     // merged with the misses, then a bulk load into a fresh arena.
     const int64_t n0 = t->n_keys, n1 = n0 + nm;
-    int64_t *ek = nullptr, *ev = nullptr;
-    uint64_t *ck = nullptr;
-    int64_t *cv = nullptr, *tmp_a = nullptr, *tmp_b = nullptr;
-    hm_tree nt = *t;  // new shape in a copy; arena swapped in at the end
-    nt.scratch = nullptr;
-    rc = shape(n1, t->cfg, &nt.height, nt.lvl_start, &nt.n_inner, &nt.n_leaf);
-    if (rc) return rc;
-    size_t off_prefix = al(nt.n_inner * nt.inner_row * 8);
-    size_t off_lrows = off_prefix + al(align_up(nt.n_inner, 4) * 4);
-    size_t off_lcnt = off_lrows + al(nt.n_leaf * nt.leaf_row * 8);
-    size_t off_lbase = off_lcnt + al(nt.n_leaf * 4);
-    size_t total = off_lbase + al(nt.n_leaf * 8);
-    int64_t tn = std::max<int64_t>(std::max<int64_t>(n1, nt.n_leaf), 1);
+    const int64_t tn = std::max<int64_t>(n1, 1);
     char *tmp = nullptr;
-    e = cudaMalloc(&nt.arena, total);
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, 6 * al(8 * tn));
-    if (e != cudaSuccess) {
-      if (nt.arena) cudaFree(nt.arena);
-      if (tmp) cudaFree(tmp);
-      return cuda_err(e);
-    }
-    ek = reinterpret_cast<int64_t *>(tmp);
-    ev = reinterpret_cast<int64_t *>(tmp + al(8 * tn));
-    ck = reinterpret_cast<uint64_t *>(tmp + 2 * al(8 * tn));
-    cv = reinterpret_cast<int64_t *>(tmp + 3 * al(8 * tn));
-    tmp_a = reinterpret_cast<int64_t *>(tmp + 4 * al(8 * tn));
-    tmp_b = reinterpret_cast<int64_t *>(tmp + 5 * al(8 * tn));
+    e = cudaMalloc(&tmp, 4 * al(8 * tn));
+    if (e != cudaSuccess) return cuda_err(e);
+    int64_t *ek = reinterpret_cast<int64_t *>(tmp);
+    int64_t *ev = reinterpret_cast<int64_t *>(tmp + al(8 * tn));
+    uint64_t *ck = reinterpret_cast<uint64_t *>(tmp + 2 * al(8 * tn));
+    int64_t *cv = reinterpret_cast<int64_t *>(tmp + 3 * al(8 * tn));
     export_contents(t, ek, ev, s);
     merge_rank_kernel<<<grid_for(n0), kThreads, 0, s>>>(ek, ev, n0, mk, nm, true, ck, cv);
     merge_rank_kernel<<<grid_for(nm), kThreads, 0, s>>>(mk, mv, nm, ek, n0, true, ck, cv);
     note_launch(2);
-    char *base = static_cast<char *>(nt.arena);
-    cudaMemsetAsync(base, 0, total, s);
-    nt.arena_bytes = total;
-    nt.inner = reinterpret_cast<int64_t *>(base);
-    nt.prefix = reinterpret_cast<int32_t *>(base + off_prefix);
-    nt.leaf_rows = reinterpret_cast<int64_t *>(base + off_lrows);
-    nt.leaf_cnt = reinterpret_cast<int32_t *>(base + off_lcnt);
-    nt.leaf_base = reinterpret_cast<int64_t *>(base + off_lbase);
-    nt.n_keys = n1;
-    rc = build_from_sorted(&nt, ck, cv, n1, tmp_a, tmp_b, s);
-    e = cudaStreamSynchronize(s);
+    rc = rebuild_from_sorted(t, ck, cv, n1, s);
     cudaFree(tmp);
-    if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
-    if (rc) {
-      cudaFree(nt.arena);
-      return rc;
-    }
-    cudaFree(t->arena);
-    t->arena = nt.arena;
-    t->arena_bytes = nt.arena_bytes;
-    t->inner = nt.inner;
-    t->prefix = nt.prefix;
-    t->leaf_rows = nt.leaf_rows;
-    t->leaf_cnt = nt.leaf_cnt;
-    t->leaf_base = nt.leaf_base;
-    t->height = nt.height;
-    std::memcpy(t->lvl_start, nt.lvl_start, sizeof(t->lvl_start));
-    t->n_inner = nt.n_inner;
-    t->n_leaf = nt.n_leaf;
-    t->n_keys = n1;
-    t->generation++;
+    if (rc) return rc;
   }
   if (t->n_keys == nm || new_ends[0] < t->key_min) t->key_min = new_ends[0];
   if (t->n_keys == nm || new_ends[1] > t->key_max) t->key_max = new_ends[1];
   return HM_OK;
+}
+
+// One epoch of deletes (no counterpart in the reference, whose
+// BPlusTree::remove is an empty stub, open-harmonia/src/bpt.cpp:771-773):
+// sort the batch and drop repeats, mark each stored key's slot, compact the
+// touched leaves in place and rescan leaf_base.  Separators stay valid (the
+// remaining keys of leaf j still lie between its separators), so the inner
+// levels are untouched.  A leaf left empty would break the invariant that
+// every leaf's first key is a key of the leaf (the bucket join searches
+// leaves by first key), so such an epoch ends in a rebuild of the remaining
+// contents instead.
+int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed_out, cudaStream_t s) {
+  if (removed_out) *removed_out = 0;
+  if (n <= 0) return HM_OK;
+  const int lc = t->cfg.leaf_cap, li = t->leaf_index, f = t->cfg.fanout;
+  const size_t s8 = al(8 * (n + 1)), s4 = al(4 * (n + 1));
+  const int64_t scan_n = std::max<int64_t>(n, t->n_leaf) + 1;
+  const size_t lb8 = al(8 * (t->n_leaf + 1));
+  size_t need = 6 * s8 + 2 * s4 + lb8 + al((int64_t)radix_scratch_bytes(n)) +
+                al((int64_t)scan_scratch_bytes(scan_n)) + 256;
+  int rc = ensure_scratch(t, need);
+  if (rc) return rc;
+  char *p = static_cast<char *>(t->scratch);
+  auto take8 = [&](void) { char *r = p; p += s8; return r; };
+  auto take4 = [&](void) { char *r = p; p += s4; return r; };
+  uint64_t *uk = reinterpret_cast<uint64_t *>(take8());
+  uint64_t *uk_alt = reinterpret_cast<uint64_t *>(take8());
+  int64_t *idx = reinterpret_cast<int64_t *>(take8());
+  int64_t *idx_alt = reinterpret_cast<int64_t *>(take8());
+  int64_t *at = reinterpret_cast<int64_t *>(take8());
+  int64_t *bk = reinterpret_cast<int64_t *>(take8());
+  int32_t *keep = reinterpret_cast<int32_t *>(take4());
+  int32_t *route = reinterpret_cast<int32_t *>(take4());
+  void *sort_scratch = p;
+  p += al((int64_t)radix_scratch_bytes(n));
+  int64_t *lbase_tmp = reinterpret_cast<int64_t *>(p);  // n_leaf + 1 entries
+  p += lb8;
+  void *scan_scratch = p;
+  p += al((int64_t)scan_scratch_bytes(scan_n));
+  unsigned long long *dremoved = reinterpret_cast<unsigned long long *>(p);
+  unsigned *dflags = reinterpret_cast<unsigned *>(p + 8);
+
+  cudaMemsetAsync(p, 0, 16, s);
+  transform_keys_in(d_keys, uk, n, s);
+  iota_kernel<<<grid_for(n), kThreads, 0, s>>>(idx, n);
+  note_launch();
+  if (radix_sort_pairs<int64_t>(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) std::swap(uk, uk_alt);
+  last_occurrence_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, n, keep, dflags);
+  exclusive_scan_i32(keep, at, n, scan_scratch, s);
+  compact_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, keep, at, n, bk);
+  note_launch(2);
+  int64_t m = 0;
+  cudaMemcpyAsync(&m, at + n, 8, cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_err(e);
+
+  delete_mark_kernel<<<grid_for(m), kThreads, 0, s>>>(t->view(), f, lc, li, bk, m, t->leaf_rows, route);
+  cudaMemsetAsync(dflags, 0, 4, s);  // the Max_Key bit of the dedup pass is not an error here
+  delete_compact_kernel<<<grid_for(m), kThreads, 0, s>>>(t->leaf_rows, t->leaf_cnt, lc, li, route, m, dremoved,
+                                                          dflags);
+  note_launch(2);
+  unsigned long long removed = 0;
+  unsigned hf = 0;
+  cudaMemcpyAsync(&removed, dremoved, 8, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&hf, dflags, 4, cudaMemcpyDeviceToHost, s);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_err(e);
+  if (removed_out) *removed_out = (int64_t)removed;
+  if (removed == 0) return HM_OK;
+  exclusive_scan_i32(t->leaf_cnt, lbase_tmp, t->n_leaf, scan_scratch, s);
+  cudaMemcpyAsync(t->leaf_base, lbase_tmp, 8 * t->n_leaf, cudaMemcpyDeviceToDevice, s);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_err(e);
+  t->n_keys -= (int64_t)removed;
+  if (!(hf & 1u)) return HM_OK;
+  // a leaf emptied: rebuild from the remaining contents
+  const int64_t n1 = t->n_keys, tn = std::max<int64_t>(n1, 1);
+  char *tmp = nullptr;
+  e = cudaMalloc(&tmp, 3 * al(8 * tn));
+  if (e != cudaSuccess) return cuda_err(e);
+  int64_t *ek = reinterpret_cast<int64_t *>(tmp);
+  int64_t *ev = reinterpret_cast<int64_t *>(tmp + al(8 * tn));
+  uint64_t *ck = reinterpret_cast<uint64_t *>(tmp + 2 * al(8 * tn));
+  export_contents(t, ek, ev, s);
+  if (n1 > 0) transform_keys_in(ek, ck, n1, s);
+  rc = rebuild_from_sorted(t, ck, ev, n1, s);
+  cudaFree(tmp);
+  return rc;
 }
 
 }  // namespace hm

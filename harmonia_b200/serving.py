@@ -14,7 +14,7 @@ import numpy as np
 from . import native
 from .native import HarmoniaError, check, lib
 
-HM_REQ_SEARCH, HM_REQ_RANGE, HM_REQ_UPSERT = 0, 1, 2
+HM_REQ_SEARCH, HM_REQ_RANGE, HM_REQ_UPSERT, HM_REQ_DELETE = 0, 1, 2, 3
 
 
 class Request(ctypes.Structure):
@@ -127,6 +127,12 @@ class Server:
         r = Request(kind=HM_REQ_UPSERT, keys=keys.ctypes.data, vals=vals.ctypes.data, n=len(keys),
                     flags=native.HM_UPSERT_REF_KEY_MINUS_1 if ref_rule else native.HM_UPSERT_SUPPLIED)
         return Ticket(self, self._submit(r), HM_REQ_UPSERT, (keys, vals), lambda: None)
+
+    def delete(self, keys) -> Ticket:
+        """Removes the stored keys among keys (an epoch barrier, like upsert)."""
+        keys = np.ascontiguousarray(np.asarray(keys, dtype=np.int64))
+        r = Request(kind=HM_REQ_DELETE, keys=keys.ctypes.data, n=len(keys))
+        return Ticket(self, self._submit(r), HM_REQ_DELETE, (keys,), lambda: None)
 
     def stats(self) -> dict:
         s = ServerStats()

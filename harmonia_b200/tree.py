@@ -189,6 +189,15 @@ class BPlusTree:
         return offsets, okeys[:m], ovals[:m]
 
     # ---- updates ----
+    def delete(self, keys, stream=None) -> int:
+        """One delete epoch: removes the stored keys among keys; returns how
+        many were removed (the reference has no working delete)."""
+        keys = _as_i64(keys)
+        removed = ctypes.c_size_t()
+        check(lib().hm_delete_batch(self._h, _ptr(keys) if len(keys) else None, len(keys),
+                                    ctypes.byref(removed), _stream_ptr(stream)), "hm_delete_batch")
+        return int(removed.value)
+
     def upsert(self, keys, values, ref_rule: bool = False, stream=None) -> None:
         keys = _as_i64(keys)
         values = _as_i64(values)
@@ -303,6 +312,12 @@ class Plan:
         if self._h is not None and self._h.value:
             check(lib().hm_plan_free(self._h), "hm_plan_free")
         self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         try:

@@ -198,17 +198,17 @@ const char *hm_strerror(int code);
  * dispatcher thread admits requests in submission order while their device
  * bytes fit the budget, coalesces consecutive reads of one kind into one
  * launch, and keeps up to `streams` launches in flight (requests arriving
- * while others run are admitted as slots and memory free up).  An upsert is
- * an epoch barrier: it applies after every earlier request and before every
- * later one, so a read returns what it would return alone against the
- * upserts submitted before it.  Every device wait is bounded
+ * while others run are admitted as slots and memory free up).  An upsert or
+ * a delete is an epoch barrier: it applies after every earlier request and
+ * before every later one, so a read returns what it would return alone
+ * against the writes submitted before it.  Every device wait is bounded
  * (device_wait_limit_ms).  No counterpart in the reference, which only runs
  * offline experiments (open-harmonia/src/main.cpp:160-417). */
-enum { HM_REQ_SEARCH = 0, HM_REQ_RANGE = 1, HM_REQ_UPSERT = 2 };
+enum { HM_REQ_SEARCH = 0, HM_REQ_RANGE = 1, HM_REQ_UPSERT = 2, HM_REQ_DELETE = 3 };
 
 typedef struct {
   int kind;              /* HM_REQ_* */
-  const int64_t *keys;   /* search: queries; range: start keys; upsert: keys (host) */
+  const int64_t *keys;   /* search: queries; range: start keys; upsert, delete: keys (host) */
   const int32_t *lens;   /* range: record counts */
   const int64_t *vals;   /* upsert: values */
   size_t n;
@@ -311,6 +311,14 @@ int hm_read_ranges(const char *path, int64_t *start, int64_t *end, size_t cap, s
 
 /* Writes keys in the same text format, one per line. */
 int hm_write_keys(const char *path, const int64_t *keys, size_t n);
+
+/* One epoch of deletes: every listed key that is stored is removed (absent
+ * keys and repeats are ignored); *removed (may be NULL) receives the count.
+ * Searches and range scans afterwards see the remaining keys only, and a later
+ * upsert can store a removed key again.  Keys may be host or device memory;
+ * returns when done.  No counterpart in the reference, whose
+ * BPlusTree::remove is an empty stub (open-harmonia/src/bpt.cpp:771-773). */
+int hm_delete_batch(hm_tree *t, const int64_t *keys, size_t n, size_t *removed, hm_stream s);
 
 /* Writes the tree's contents (keys in order with their values) and its
  * configuration to a binary file, with a checksum.  No counterpart in the

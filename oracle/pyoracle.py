@@ -182,6 +182,14 @@ def upsert_set(skeys, svals, bkeys, bvals, ref_rule: bool = False):
 _ref = None
 
 
+def delete_set(skeys, svals, dkeys):
+    """Contents after removing dkeys (set semantics; the reference's remove
+    is an empty stub, open-harmonia/src/bpt.cpp:771-773, so this is the
+    specification, not a restatement)."""
+    keep = ~np.isin(skeys, np.asarray(dkeys, np.int64))
+    return skeys[keep], svals[keep]
+
+
 def _ref_lib():
     global _ref
     if _ref is None:
