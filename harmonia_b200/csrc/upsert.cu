@@ -145,13 +145,16 @@ __global__ void merge_leaf_kernel(int64_t *leaf_rows, int32_t *leaf_cnt, int lc,
                                   const int32_t *__restrict__ is_start,
                                   const int64_t *__restrict__ run_start,
                                   const int32_t *__restrict__ run_len,
-                                  const int32_t *__restrict__ run_leaf, int64_t nm) {
+                                  const int32_t *__restrict__ run_leaf, int64_t nm,
+                                  const int32_t *__restrict__ run_parent = nullptr,
+                                  const int32_t *__restrict__ mark = nullptr) {
   __shared__ int64_t sk[kThreads / 32][128];
   __shared__ int64_t sv[kThreads / 32][128];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + w; i < nm; i += warps) {
     if (!is_start[i]) continue;
+    if (mark && mark[run_parent[i]]) continue;  // its subtree is rebalanced instead
     const int32_t leaf = run_leaf[i];
     const int64_t r0 = run_start[i];
     const int rl = run_len[i];
@@ -187,6 +190,146 @@ __global__ void merge_leaf_kernel(int64_t *leaf_rows, int32_t *leaf_cnt, int lc,
     if (lane == 0) leaf_cnt[leaf] = nc;
     __syncwarp();
   }
+}
+
+// ---- subtree rebalancing (an epoch whose new keys overflow a leaf) ----
+//
+// The subtree of a last-level inner node p is its children leaves [a, b].
+// When a leaf overflows but p's subtree still has room for its keys and all
+// the epoch's new keys routed into it, the subtree's keys are re-spread
+// evenly over the same leaves and p's separators rewritten; nothing outside
+// the subtree changes (p's own separator in its parent stays a valid fence,
+// because every new key routed here is at least that separator).  Only when
+// some subtree has no room is the whole tree rebuilt.
+
+struct Subtree {
+  int64_t lvl0, lvl1;  // last inner level: nodes [lvl0, lvl1); lvl1 == n_inner
+  int64_t n_inner, n_leaf;
+};
+
+__device__ __forceinline__ int64_t first_miss_at_or_after(const int32_t *__restrict__ ml, int64_t nm, int64_t leaf) {
+  int64_t lo = 0, hi = nm;  // first miss whose leaf >= leaf
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (ml[mid] < leaf) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void subtree_leaves(const int32_t *__restrict__ prefix, const Subtree &g, int64_t p,
+                                               int64_t *a, int64_t *b) {
+  const int64_t c0 = prefix[p];
+  const int64_t c1 = p + 1 < g.lvl1 ? prefix[p + 1] : g.n_inner + g.n_leaf;
+  *a = c0 - g.n_inner;
+  *b = c1 - 1 - g.n_inner;
+}
+
+// One thread per run of misses: its leaf's parent (run_parent, as an index
+// into the last level); an overflowing leaf marks its parent when the
+// subtree has room, else flags bit2 (rebuild the tree).
+__global__ void subtree_mark_kernel(const int32_t *__restrict__ prefix, const int32_t *__restrict__ leaf_cnt,
+                                    const int64_t *__restrict__ leaf_base, int lc, Subtree g,
+                                    const int32_t *__restrict__ is_start, const int32_t *__restrict__ run_len,
+                                    const int32_t *__restrict__ run_leaf, const int32_t *__restrict__ ml,
+                                    int64_t nm, int32_t *__restrict__ run_parent, int32_t *__restrict__ mark,
+                                    unsigned *flags) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (!is_start[i]) continue;
+    const int64_t leaf = run_leaf[i];
+    int64_t lo = g.lvl0, hi = g.lvl1 - 1;  // last node p with prefix[p] <= the leaf's id
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= g.n_inner + leaf) lo = mid; else hi = mid - 1;
+    }
+    run_parent[i] = (int32_t)(lo - g.lvl0);
+    if (leaf_cnt[leaf] + run_len[i] <= lc) continue;
+    int64_t a, b;
+    subtree_leaves(prefix, g, lo, &a, &b);
+    const int64_t keys = leaf_base[b] + leaf_cnt[b] - leaf_base[a];
+    const int64_t adds = first_miss_at_or_after(ml, nm, b + 1) - first_miss_at_or_after(ml, nm, a);
+    if (keys + adds <= (b - a + 1) * (int64_t)lc) {
+      mark[lo - g.lvl0] = 1;
+    } else {
+      atomicOr(flags, 4u);
+    }
+  }
+}
+
+// One CTA per last-level node; marked ones are rebalanced.  The existing
+// records are gathered into shared memory first, then every element (old or
+// new) is written to its place in the merged order, spread evenly over the
+// subtree's leaves (leaf jj gets positions [part_start(jj), part_start(jj+1))).
+__global__ void subtree_rebalance_kernel(int64_t *inner, const int32_t *__restrict__ prefix, int64_t *leaf_rows,
+                                         int32_t *leaf_cnt, const int64_t *__restrict__ leaf_base, int f, int lc,
+                                         int li, Subtree g, const int32_t *__restrict__ mark,
+                                         const int64_t *__restrict__ mk, const int64_t *__restrict__ mv,
+                                         const int32_t *__restrict__ ml, int64_t nm) {
+  extern __shared__ __align__(16) longlong2 staged[];  // the subtree's existing records
+  if (!mark[blockIdx.x]) return;
+  const int64_t p = g.lvl0 + blockIdx.x;
+  int64_t a, b;
+  subtree_leaves(prefix, g, p, &a, &b);
+  const int64_t nl = b - a + 1, row = li + 2 * lc;
+  const int64_t base = leaf_base[a];
+  const int64_t K = leaf_base[b] + leaf_cnt[b] - base;
+  const int64_t m0 = first_miss_at_or_after(ml, nm, a), m1 = first_miss_at_or_after(ml, nm, b + 1);
+  const int64_t M = m1 - m0, T = K + M;
+  for (int64_t x = threadIdx.x; x < nl * lc; x += blockDim.x) {
+    const int64_t j = a + x / lc, sl = x % lc;
+    if (sl < leaf_cnt[j]) {
+      const int64_t *r = leaf_rows + j * row + li;
+      staged[leaf_base[j] - base + sl] = make_longlong2(r[sl], r[lc + sl]);
+    }
+  }
+  __syncthreads();
+  const int64_t q = T / nl, rem = T % nl;
+  auto put = [&](int64_t pos, int64_t k, int64_t v) {
+    const int64_t jj = pos < rem * (q + 1) ? pos / (q + 1) : rem + (pos - rem * (q + 1)) / q;
+    const int64_t sl = pos - part_start(jj, T, nl);
+    int64_t *r = leaf_rows + (a + jj) * row + li;
+    r[sl] = k;
+    r[lc + sl] = v;
+  };
+  for (int64_t e = threadIdx.x; e < K; e += blockDim.x) {  // old record: own index + new keys below it
+    const int64_t k = staged[e].x;
+    int64_t lo = m0, hi = m1;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (mk[mid] < k) lo = mid + 1; else hi = mid;
+    }
+    put(e + (lo - m0), k, staged[e].y);
+  }
+  for (int64_t i = threadIdx.x; i < M; i += blockDim.x) {  // new key: own index + old keys below it
+    const int64_t k = mk[m0 + i];
+    int64_t lo = 0, hi = K;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (staged[mid].x < k) lo = mid + 1; else hi = mid;
+    }
+    put(i + lo, k, mv[m0 + i]);
+  }
+  for (int64_t x = threadIdx.x; x < nl * lc; x += blockDim.x) {  // padding and counts
+    const int64_t jj = x / lc, sl = x % lc;
+    const int64_t len = part_start(jj + 1, T, nl) - part_start(jj, T, nl);
+    if (sl >= len) {
+      int64_t *r = leaf_rows + (a + jj) * row + li;
+      r[sl] = kMaxKey;
+      r[lc + sl] = HM_NOT_FOUND;
+    }
+    if (sl == 0) leaf_cnt[a + jj] = (int32_t)len;
+  }
+  __syncthreads();
+  for (int64_t x = threadIdx.x; x < nl * li; x += blockDim.x) {  // 64-key leaves: index words
+    const int64_t jj = x / li, w = x % li;
+    int64_t *r = leaf_rows + (a + jj) * row;
+    r[w] = 8 * (w + 1) < lc ? r[li + 8 * (w + 1)] : kMaxKey;
+  }
+  int64_t *pr = inner + p * (f / 8 + f);
+  for (int sidx = threadIdx.x; sidx < f; sidx += blockDim.x)  // separators: first key of child s + 1
+    pr[f / 8 + sidx] = sidx < nl - 1 ? leaf_rows[(a + sidx + 1) * row + li] : kMaxKey;
+  __syncthreads();
+  for (int w = threadIdx.x; w < f / 8; w += blockDim.x) pr[w] = 8 * (w + 1) < f ? pr[f / 8 + 8 * (w + 1)] : kMaxKey;
 }
 
 // Merge of two sorted, disjoint runs: out slot = own index + rank in the other run.
@@ -337,7 +480,8 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   // the leaf_base rescan covers every leaf, not just the batch
   const int64_t scan_n = std::max<int64_t>(n, t->n_leaf) + 1;
   const size_t lb8 = al(8 * (t->n_leaf + 1));
-  size_t need = 9 * s8 + 7 * s4 + lb8 + al((int64_t)radix_scratch_bytes(n)) +
+  const size_t mk4 = al(4 * (t->n_inner + 1));  // subtree marks, one per last-level node
+  size_t need = 9 * s8 + 7 * s4 + lb8 + mk4 + al((int64_t)radix_scratch_bytes(n)) +
                 al((int64_t)scan_scratch_bytes(scan_n)) + 256;
   int rc = ensure_scratch(t, need);
   if (rc) return rc;
@@ -367,6 +511,8 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   p += lb8;
   void *scan_scratch = p;
   p += al((int64_t)scan_scratch_bytes(scan_n));
+  int32_t *marks = reinterpret_cast<int32_t *>(p);
+  p += mk4;
   unsigned *dflags = reinterpret_cast<unsigned *>(p);
 
   cudaMemsetAsync(dflags, 0, 8, s);
@@ -413,16 +559,48 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_err(e);
 
-  if (!(hf & 1u)) {
-    // Every touched leaf has room: merge in place.
+  // Some leaf overflows: rebalance the subtrees (last-level nodes) that have
+  // room; if one has none, rebuild the tree.
+  int32_t *mark = nullptr, *run_parent = nullptr;
+  const Subtree g{t->lvl_start[t->height - 1], t->n_inner, t->n_inner, t->n_leaf};
+  const int64_t last_nodes = g.lvl1 - g.lvl0;
+  if (hf & 1u) {
+    run_parent = keep;  // free after the batch compaction; nm <= n entries
+    mark = marks;
+    cudaMemsetAsync(mark, 0, 4 * last_nodes, s);
+    subtree_mark_kernel<<<grid_for(nm), kThreads, 0, s>>>(t->prefix, t->leaf_cnt, t->leaf_base, lc, g, is_start,
+                                                           run_len, run_leaf, ml, nm, run_parent, mark, dflags);
+    note_launch();
+    e = cudaMemcpyAsync(&hf, dflags, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_err(e);
+  }
+  if (!(hf & 4u)) {
+    // Every touched leaf has room, or its subtree does: merge in place.
     int64_t blocks = (nm + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
     merge_leaf_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(t->leaf_rows, t->leaf_cnt, lc,
                                                             li, mk, mv, is_start, run_start, run_len,
-                                                            run_leaf, nm);
+                                                            run_leaf, nm, run_parent, mark);
+    note_launch();
+    if (hf & 1u) {
+      const size_t smem = (size_t)t->cfg.fanout * lc * sizeof(longlong2);
+      static bool attr_set = false;  // up to 128 KiB (fanout 128, 64-key leaves)
+      if (!attr_set) {
+        e = cudaFuncSetAttribute(subtree_rebalance_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 128 * 64 * (int)sizeof(longlong2));
+        if (e != cudaSuccess) return cuda_err(e);
+        attr_set = true;
+      }
+      subtree_rebalance_kernel<<<(unsigned)last_nodes, kThreads, smem, s>>>(
+          t->inner, t->prefix, t->leaf_rows, t->leaf_cnt, t->leaf_base, t->cfg.fanout, lc, li, g, mark, mk, mv, ml,
+          nm);
+      note_launch();
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_err(e);
+    }
     exclusive_scan_i32(t->leaf_cnt, lbase_tmp, t->n_leaf, scan_scratch, s);
     cudaMemcpyAsync(t->leaf_base, lbase_tmp, 8 * t->n_leaf, cudaMemcpyDeviceToDevice, s);
-    note_launch();
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_err(e);
     t->n_keys += nm;

@@ -116,3 +116,52 @@ def test_tiny_batches_on_a_large_tree():
         got = t.range_search(st, ln)
         exp = po.PortTree(sk, sv).range(st, ln)
         assert all((a == b).all() for a, b in zip(got, exp))
+
+
+@pytest.mark.parametrize("fanout,leaf_cap,fill", [(64, 16, 12), (128, 64, 48), (64, 64, 40)])
+def test_overflowing_leaf_rebalances_its_subtree(fanout, leaf_cap, fill):
+    # new keys packed into one leaf's key range overflow it while its subtree
+    # (the last-level inner node's leaves) still has room: the subtree is
+    # re-spread in place, the arena and the leaf count stay, plans need no
+    # re-capture, and every read matches the oracle
+    keys = dg.gen_keys(1 << 17, seed=61)
+    sk = np.sort(keys)
+    sv = dg.values_for(sk)
+    with BPlusTree.bulk_load(keys, dg.values_for(keys), fanout=fanout, leaf_cap=leaf_cap, leaf_fill=fill) as t:
+        info0 = t.info()
+        q = dg.gen_point_queries(sk, 1 << 15, 0.8, seed=62)
+        dq, dout = cuda(q), torch.empty(len(q), dtype=torch.int64, device="cuda")
+        with t.plan([(dq, dout)]) as plan:
+            ek, ev = sk, sv
+            for epoch, at in enumerate((5000, 5000, 70000)):
+                j = at + int(np.argmax(np.diff(ek[at:at + 40])))  # the widest gap near `at`
+                lo, hi = int(ek[j]), int(ek[j + 1])
+                room = leaf_cap - fill + 3
+                new = np.unique(lo + 1 + (np.arange(room) * max(1, (hi - lo - 1) // (room + 1))))
+                new = new[(new > lo) & (new < hi)]
+                assert len(new) > leaf_cap - fill, "the gap must hold enough keys to overflow a leaf"
+                upd = ek[j - 3: j]
+                bk = np.concatenate([new, upd])
+                bv = bk * 3 + epoch
+                t.upsert(bk, bv)
+                ek, ev = po.upsert_set(ek, ev, bk, bv)
+                info = t.info()
+                assert info.n_leaf == info0.n_leaf and info.leaf_rows == info0.leaf_rows  # no rebuild
+                xk, xv = t.export()
+                assert (xk == ek).all() and (xv == ev).all()
+                oracle = po.PortTree(ek, ev)
+                q2 = np.concatenate([bk, q])
+                assert (t.search(cuda(q2)).cpu().numpy() == oracle.search(q2)).all()
+                st, ln = dg.gen_ranges(2000, 1, 200, seed=63 + epoch)
+                st[:50] = bk[:50] if len(bk) >= 50 else st[:50]
+                got = t.range_search(st, ln)
+                exp = oracle.range(st, ln)
+                assert all((a == b).all() for a, b in zip(got, exp))
+                plan.launch()
+                torch.cuda.synchronize()
+                assert (dout.cpu().numpy() == oracle.search(q)).all()
+            # the join over rebalanced leaves (first keys must still order the leaves)
+            t.set_search_config(join=1)
+            big = dg.gen_point_queries(ek, 1 << 19, 0.9, seed=70)
+            assert (t.search(cuda(big)).cpu().numpy() == po.PortTree(ek, ev).search(big)).all()
+            t.set_search_config(join=-1)
