@@ -241,8 +241,12 @@ __device__ __forceinline__ void search_tile(const DevTree &t, const int64_t *sro
   }
 }
 
+#ifndef HM_SEARCH_MINB
+#define HM_SEARCH_MINB 6  // resident CTAs per SM the register budget must allow (measured: 6 beats 1 and 8)
+#endif
+
 template <int W, int F, int LC, int Q>
-__global__ void __launch_bounds__(kThreads) search_kernel(Args a) {
+__global__ void __launch_bounds__(kThreads, (Q <= 2 ? HM_SEARCH_MINB : 1)) search_kernel(Args a) {
   extern __shared__ __align__(128) unsigned char smem[];
   constexpr int ROW = F / 8 + F;
   constexpr int TILE = (kThreads / W) * Q;
