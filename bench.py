@@ -303,9 +303,10 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
     """Serving workload: a 2^25-key tree; Poisson arrivals, request sizes
     log-uniform in [64, 2^20]; 90% point search (80% hits), 5% range (length
     1..128), 5% upsert (half new, half existing keys) applied in epochs.
-    Offered loads are fractions of the measured capacity of back-to-back
-    point requests; reports throughput and p50/p99 submit-to-completion
-    latency at each load, and checks a sample of answers."""
+    Offered loads are fractions of the measured capacity for the same mix
+    submitted back to back; reports throughput and p50/p99
+    submit-to-completion latency at each load, and checks a sample of
+    answers."""
     import threading
     from harmonia_b200 import BPlusTree, datagen as dg
     from harmonia_b200.serving import Server
@@ -320,17 +321,39 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
     with Server(tree, streams=3, max_launch_queries=1 << 22, device_budget_bytes=2 << 30) as srv:
         def sizes(k):
             return np.exp(rng.uniform(np.log(64), np.log(1 << 20), k)).astype(np.int64)
-        # capacity: back-to-back point requests of the same size law
-        cap_sizes = sizes(200)
-        offs = rng.integers(0, len(pool) - (1 << 20), 200)
+
+        new_keys = dg.gen_keys(1 << 22, seed + 100)
+        new_at = [0]
+
+        def submit(kind_u, m):
+            """One request of the mix: 90% point, 5% range, 5% upsert."""
+            if kind_u < 0.90:
+                o = int(rng.integers(0, len(pool) - m))
+                return ("s", srv.search(pool[o:o + m]), o, m)
+            if kind_u < 0.95:
+                k = max(1, m // 64)
+                o = int(rng.integers(0, len(rstart) - k))
+                return ("r", srv.range(rstart[o:o + k], rlen[o:o + k]), o, k)
+            k = max(2, min(m // 16, 64))
+            nk = new_keys[new_at[0]:new_at[0] + k // 2]
+            new_at[0] += k // 2
+            ek = keys[rng.integers(0, n, k - k // 2)]
+            bk = np.concatenate([nk, ek])
+            bv = np.concatenate([dg.values_for(nk), ek - 1])
+            return ("u", srv.upsert(bk, bv), 0, k)
+
+        # capacity: the same mix submitted back to back
+        cap_n = 400
+        cap_kinds, cap_sizes = rng.random(cap_n), sizes(cap_n)
         t0 = time.perf_counter()
-        tks = [srv.search(pool[o:o + m]) for o, m in zip(offs, cap_sizes)]
+        tks = [submit(u, int(m)) for u, m in zip(cap_kinds, cap_sizes)]
         for tk in tks:
-            tk.wait()
-        cap_qps = cap_sizes.sum() / (time.perf_counter() - t0)
-        mean_size = float(np.exp(np.log(1 << 20) - np.log(64)) - 1) * 64 / np.log((1 << 20) / 64)
+            tk[1].wait()
+        cap_wall = time.perf_counter() - t0
+        cap_rps = cap_n / cap_wall
+        cap_qps = srv.stats()["queries"] / cap_wall
         for frac in loads:
-            rate = frac * cap_qps / mean_size  # requests per second
+            rate = frac * cap_rps  # requests per second
             srv.reset_stats()
             count = int(rate * seconds) + 1
             gaps = rng.exponential(1.0 / rate, count)
@@ -339,26 +362,11 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
             tickets = []
             t_start = time.perf_counter()
             due = t_start
-            new_keys = dg.gen_keys(count * 64, seed + 100 + int(frac * 100))
             for i in range(count):
                 due += gaps[i]
                 while time.perf_counter() < due:
                     pass
-                m = int(szs[i])
-                if kinds[i] < 0.90:
-                    o = int(rng.integers(0, len(pool) - m))
-                    tickets.append(("s", srv.search(pool[o:o + m]), o, m))
-                elif kinds[i] < 0.95:
-                    k = max(1, m // 64)
-                    o = int(rng.integers(0, len(rstart) - k))
-                    tickets.append(("r", srv.range(rstart[o:o + k], rlen[o:o + k]), o, k))
-                else:
-                    k = max(2, min(m // 16, 64))
-                    nk = new_keys[i * 64:i * 64 + k // 2]
-                    ek = keys[rng.integers(0, n, k - k // 2)]
-                    bk = np.concatenate([nk, ek])
-                    bv = np.concatenate([dg.values_for(nk), ek - 1])
-                    tickets.append(("u", srv.upsert(bk, bv), 0, k))
+                tickets.append(submit(kinds[i], int(szs[i])))
             for kind, tk, o, m in tickets:
                 tk.wait()
             wall = time.perf_counter() - t_start
@@ -375,7 +383,8 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
             got = tk._result()
             ok = (got == -1) | (got == dg.values_for(q)) | (got == q - 1)
             assert ok.all(), "serving answer outside the possible values"
-        out["capacity_mqps"] = round(cap_qps / 1e6, 1)
+        out["capacity"] = {"req_per_s": round(cap_rps, 1), "mqps": round(cap_qps / 1e6, 1),
+                           "what": "the same request mix submitted back to back; loads are fractions of it"}
     tree.close()
     return out
 

@@ -63,6 +63,85 @@ struct Slot {
   Clock::time_point t_launch;
 };
 
+// Host copies between the callers' buffers and the slots' pinned staging run
+// on a few helper threads besides the dispatcher: one thread's memcpy is far
+// below the host's memory bandwidth and caps the serving rate.
+struct CopyJob {
+  char *dst;
+  const char *src;
+  size_t bytes;
+};
+
+class CopyPool {
+ public:
+  void start(int helpers) {
+    for (int i = 0; i < helpers; i++) th_.emplace_back([this] { work(); });
+  }
+  void stop() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      quit_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : th_) t.join();
+    th_.clear();
+  }
+  // Runs every copy (split into 1 MiB pieces) on the helpers and the calling
+  // thread; returns when all are done.  One caller at a time.
+  void run(const std::vector<CopyJob> &jobs) {
+    size_t total = 0;
+    for (const CopyJob &j : jobs) total += j.bytes;
+    if (th_.empty() || total < kPiece) {
+      for (const CopyJob &j : jobs) std::memcpy(j.dst, j.src, j.bytes);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      pieces_.clear();
+      for (const CopyJob &j : jobs)
+        for (size_t o = 0; o < j.bytes; o += kPiece)
+          pieces_.push_back({j.dst + o, j.src + o, std::min(kPiece, j.bytes - o)});
+      next_ = 0;
+      left_ = pieces_.size();
+    }
+    cv_.notify_all();
+    for (;;) {
+      CopyJob j;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (next_ >= pieces_.size()) break;
+        j = pieces_[next_++];
+      }
+      std::memcpy(j.dst, j.src, j.bytes);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--left_ == 0) cv_done_.notify_all();
+    }
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_done_.wait(lk, [this] { return left_ == 0; });
+  }
+
+ private:
+  static constexpr size_t kPiece = (size_t)1 << 20;
+  void work() {
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_.wait(lk, [this] { return quit_ || next_ < pieces_.size(); });
+      if (quit_) return;
+      const CopyJob j = pieces_[next_++];
+      lk.unlock();
+      std::memcpy(j.dst, j.src, j.bytes);
+      lk.lock();
+      if (--left_ == 0) cv_done_.notify_all();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable cv_, cv_done_;
+  std::vector<CopyJob> pieces_;
+  size_t next_ = 0, left_ = 0;
+  bool quit_ = false;
+  std::vector<std::thread> th_;
+};
+
 size_t req_device_bytes(const hm_request &r) {
   switch (r.kind) {
     case HM_REQ_SEARCH: return 16 * r.n;
@@ -93,6 +172,7 @@ struct hm_server {
   std::thread th;
   std::vector<Slot> slots;
   size_t reserved = 0;
+  CopyPool copies;
   // stats
   std::vector<double> lat;
   uint64_t completed = 0, rejected = 0, launches = 0, epochs = 0, queries = 0, failed = 0;
@@ -148,10 +228,12 @@ int launch_points(hm_server *sv, Slot &sl) {
   if (rc) return rc;
   int64_t *hq = reinterpret_cast<int64_t *>(sl.pin);
   int64_t o = 0;
+  std::vector<CopyJob> jobs;
   for (Req *q : sl.reqs) {
-    std::memcpy(hq + o, q->r.keys, q->r.n * 8);
+    jobs.push_back({reinterpret_cast<char *>(hq + o), reinterpret_cast<const char *>(q->r.keys), q->r.n * 8});
     o += (int64_t)q->r.n;
   }
+  sv->copies.run(jobs);
   int64_t *dq = reinterpret_cast<int64_t *>(sl.dev);
   int64_t *dout = reinterpret_cast<int64_t *>(sl.dev + qb);
   cudaError_t e = cudaMemcpyAsync(dq, hq, n * 8, cudaMemcpyHostToDevice, sl.s);
@@ -168,11 +250,13 @@ void complete_points(hm_server *sv, Slot &sl) {
   const size_t qb = align_up(sl.n * 8, 256);
   const int64_t *hout = reinterpret_cast<const int64_t *>(sl.pin + qb);
   int64_t o = 0;
+  std::vector<CopyJob> jobs;
   for (Req *q : sl.reqs) {
-    std::memcpy(q->r.out, hout + o, q->r.n * 8);
+    jobs.push_back({reinterpret_cast<char *>(q->r.out), reinterpret_cast<const char *>(hout + o), q->r.n * 8});
     o += (int64_t)q->r.n;
-    finish(sv, q, HM_OK);
   }
+  sv->copies.run(jobs);
+  for (Req *q : sl.reqs) finish(sv, q, HM_OK);
 }
 
 // Coalesced range requests: locate + scan + copy on the slot's stream, the
@@ -320,11 +404,14 @@ void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
     int64_t *hk = reinterpret_cast<int64_t *>(sl.pin);
     int64_t *hv = reinterpret_cast<int64_t *>(sl.pin + b);
     int64_t o = 0;
+    std::vector<CopyJob> jobs;
     for (Req *q : ups) {
-      std::memcpy(hk + o, q->r.keys, q->r.n * 8);
-      if (!del) std::memcpy(hv + o, q->r.vals, q->r.n * 8);
+      jobs.push_back({reinterpret_cast<char *>(hk + o), reinterpret_cast<const char *>(q->r.keys), q->r.n * 8});
+      if (!del)
+        jobs.push_back({reinterpret_cast<char *>(hv + o), reinterpret_cast<const char *>(q->r.vals), q->r.n * 8});
       o += (int64_t)q->r.n;
     }
+    sv->copies.run(jobs);
     int64_t *dk = reinterpret_cast<int64_t *>(sl.dev);
     int64_t *dv = reinterpret_cast<int64_t *>(sl.dev + b);
     cudaError_t e = cudaMemcpyAsync(dk, hk, n * 8, cudaMemcpyHostToDevice, sl.s);
@@ -532,6 +619,8 @@ int hm_server_start(hm_tree *t, const hm_server_config *cfg, hm_server **out) {
     }
   }
   sv->t_start = Clock::now();
+  const unsigned hw = std::thread::hardware_concurrency();
+  sv->copies.start((int)std::min(8u, std::max(1u, hw / 4)));
   sv->th = std::thread(dispatcher, sv);
   *out = sv;
   return HM_OK;
@@ -635,6 +724,7 @@ int hm_server_stop(hm_server *sv) {
   }
   for (Req *q : cancelled) finish(sv, q, HM_ECANCELLED);
   if (sv->th.joinable()) sv->th.join();
+  sv->copies.stop();
   return HM_OK;
 }
 

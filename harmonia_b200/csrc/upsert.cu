@@ -76,6 +76,80 @@ __global__ void compact_batch_kernel(const uint64_t *__restrict__ uk, const int6
   }
 }
 
+// Small batches (the serving loop's epochs) skip the multi-pass radix sort:
+// one CTA sorts (key, input index) pairs in shared memory with a bitonic
+// network, keeps each key's last occurrence and writes the kept keys (and
+// values) in key order to bk/bv and their number to *count; flags bit1 if a
+// key equals Max_Key.
+constexpr int kSmallSort = 2048;
+
+__global__ void __launch_bounds__(1024) small_sort_unique_kernel(const int64_t *__restrict__ keys,
+                                                                 const int64_t *__restrict__ vals, int n,
+                                                                 int64_t *__restrict__ bk, int64_t *__restrict__ bv,
+                                                                 int64_t *__restrict__ count, unsigned *flags) {
+  __shared__ uint64_t sk[kSmallSort];
+  __shared__ int32_t si[kSmallSort];
+  __shared__ int32_t wsum[32];
+  const int tid = threadIdx.x;
+  int P = 1;
+  while (P < n) P <<= 1;
+  unsigned f = 0;
+  for (int i = tid; i < P; i += blockDim.x) {
+    const bool real = i < n;
+    const int64_t k = real ? keys[i] : 0;
+    if (real && k == kMaxKey) f |= 2u;
+    sk[i] = real ? (uint64_t)k ^ kSign : ~0ull;  // padding sorts after every real key
+    si[i] = real ? i : INT32_MAX;
+  }
+  if (f) atomicOr(flags, f);
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < P; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const bool asc = (i & k) == 0;
+          const bool gt = sk[i] > sk[ixj] || (sk[i] == sk[ixj] && si[i] > si[ixj]);
+          if (gt == asc) {
+            const uint64_t tk = sk[i];
+            sk[i] = sk[ixj];
+            sk[ixj] = tk;
+            const int32_t ti = si[i];
+            si[i] = si[ixj];
+            si[ixj] = ti;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // keep the last occurrence of each key; two elements per thread, block scan
+  int kept[2], mine = 0;
+  for (int h = 0; h < 2; h++) {
+    const int i = 2 * tid + h;
+    kept[h] = i < n && (i == n - 1 || sk[i] != sk[i + 1]);
+    mine += kept[h];
+  }
+  int incl = mine;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if ((tid & 31) >= o) incl += y;
+  }
+  if ((tid & 31) == 31) wsum[tid >> 5] = incl;
+  __syncthreads();
+  int before = incl - mine;
+  for (int w = 0; w < (tid >> 5); w++) before += wsum[w];
+  for (int h = 0; h < 2; h++) {
+    const int i = 2 * tid + h;
+    if (kept[h]) {
+      bk[before] = (int64_t)(sk[i] ^ kSign);
+      if (bv) bv[before] = vals[si[i]];
+      before++;
+    }
+  }
+  if (tid == blockDim.x - 1) *count = before;
+}
+
 // Hits are updated in place; misses get miss[i] = 1 and their leaf.
 __global__ void apply_kernel(DevTree t, int f, int lc, int li, int flags,
                              const int64_t *__restrict__ bk, const int64_t *__restrict__ bv, int64_t m,
@@ -516,18 +590,23 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   unsigned *dflags = reinterpret_cast<unsigned *>(p);
 
   cudaMemsetAsync(dflags, 0, 8, s);
-  transform_keys_in(d_keys, uk, n, s);
-  iota_kernel<<<grid_for(n), kThreads, 0, s>>>(idx, n);
-  note_launch();
-  if (radix_sort_pairs<int64_t>(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) {
-    std::swap(uk, uk_alt);
-    std::swap(idx, idx_alt);
+  if (n <= kSmallSort) {
+    small_sort_unique_kernel<<<1, 1024, 0, s>>>(d_keys, d_vals, (int)n, bk, bv, at + n, dflags);
+    note_launch();
+  } else {
+    transform_keys_in(d_keys, uk, n, s);
+    iota_kernel<<<grid_for(n), kThreads, 0, s>>>(idx, n);
+    note_launch();
+    if (radix_sort_pairs<int64_t>(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) {
+      std::swap(uk, uk_alt);
+      std::swap(idx, idx_alt);
+    }
+    last_occurrence_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, n, keep, dflags);
+    exclusive_scan_i32(keep, at, n, scan_scratch, s);
+    compact_batch_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, idx, d_vals, keep, at, n, bk, bv);
+    note_launch(2);
   }
   run_start = idx_alt;
-  last_occurrence_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, n, keep, dflags);
-  exclusive_scan_i32(keep, at, n, scan_scratch, s);
-  compact_batch_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, idx, d_vals, keep, at, n, bk, bv);
-  note_launch(2);
   int64_t hm_[2] = {0, 0};
   unsigned hf = 0;
   cudaMemcpyAsync(&hm_[0], at + n, 8, cudaMemcpyDeviceToHost, s);
@@ -670,14 +749,19 @@ int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed_
   unsigned *dflags = reinterpret_cast<unsigned *>(p + 8);
 
   cudaMemsetAsync(p, 0, 16, s);
-  transform_keys_in(d_keys, uk, n, s);
-  iota_kernel<<<grid_for(n), kThreads, 0, s>>>(idx, n);
-  note_launch();
-  if (radix_sort_pairs<int64_t>(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) std::swap(uk, uk_alt);
-  last_occurrence_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, n, keep, dflags);
-  exclusive_scan_i32(keep, at, n, scan_scratch, s);
-  compact_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, keep, at, n, bk);
-  note_launch(2);
+  if (n <= kSmallSort) {
+    small_sort_unique_kernel<<<1, 1024, 0, s>>>(d_keys, nullptr, (int)n, bk, nullptr, at + n, dflags);
+    note_launch();
+  } else {
+    transform_keys_in(d_keys, uk, n, s);
+    iota_kernel<<<grid_for(n), kThreads, 0, s>>>(idx, n);
+    note_launch();
+    if (radix_sort_pairs<int64_t>(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) std::swap(uk, uk_alt);
+    last_occurrence_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, n, keep, dflags);
+    exclusive_scan_i32(keep, at, n, scan_scratch, s);
+    compact_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, keep, at, n, bk);
+    note_launch(2);
+  }
   int64_t m = 0;
   cudaMemcpyAsync(&m, at + n, 8, cudaMemcpyDeviceToHost, s);
   cudaError_t e = cudaStreamSynchronize(s);
