@@ -507,6 +507,17 @@ def main():
                 "kernel_ms": round(kernel_ms, 4),
                 "path_ms": round(sum(v[1] / max(v[0], 1) for v in stages.values()), 4)}
 
+    # comparison kernel: HB+-style pointer-chasing descent (one thread per query)
+    if args.extras:
+        for _ in range(args.warmup):
+            tree.search_pointer_baseline(d_q, d_out)
+        pb_ms = timed(args.steps, lambda: tree.search_pointer_baseline(d_q, d_out))
+        assert (d_out[:4096].cpu().numpy() == exp).all(), "pointer baseline results are wrong"
+        extras["pointer_baseline"] = {"value": round(ws * m / pb_ms / 1e3, 1), "unit": UNIT,
+                                      "ms_per_step": round(pb_ms, 4),
+                                      "what": "HB+-style descent following per-node child ids, one thread per "
+                                              "query, no prefix array, no pre-sort (comparison kernel)"}
+
     # pre-sorted input (the batch arrives partially sorted by its top 16 key bits)
     if args.extras:
         order = np.argsort(q >> np.int64(47), kind="stable")

@@ -156,6 +156,7 @@ int free_tree(hm_tree *t) {
   if (!t) return HM_OK;
   cudaDeviceSynchronize();
   if (t->arena) cudaFree(t->arena);
+  if (t->child_ids) cudaFree(t->child_ids);
   if (t->scratch) cudaFree(t->scratch);
   if (t->d_err) cudaFree(t->d_err);
   if (t->pinned) cudaFreeHost(t->pinned);

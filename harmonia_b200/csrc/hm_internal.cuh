@@ -113,6 +113,9 @@ struct hm_tree {
   int64_t key_min = 0, key_max = 0;  // for the pre-sort digit
   uint64_t generation = 0;           // bumped when the arena is rebuilt
   int64_t join_tuned_min = INT64_MAX;  // smallest batch the autotuner saw the join win
+  // comparison baseline (hm_search_baseline): children ids per inner node
+  int32_t *child_ids = nullptr;
+  uint64_t child_ids_generation = ~0ull;
   // arena
   void *arena = nullptr;
   size_t arena_bytes = 0;

@@ -29,7 +29,7 @@ EXPORTS = (
     "hm_search_noalloc", "hm_server_config_default", "hm_server_start", "hm_server_submit",
     "hm_server_wait", "hm_server_get_stats", "hm_server_reset_stats", "hm_server_stop", "hm_server_free",
     "hm_last_cuda_error", "hm_read_keys", "hm_read_ranges", "hm_write_keys", "hm_snapshot_save",
-    "hm_snapshot_load", "hm_delete_batch",
+    "hm_snapshot_load", "hm_delete_batch", "hm_search_baseline",
 )
 HM_NOALLOC_MAX_QUERIES = 1 << 20
 
@@ -121,6 +121,7 @@ def lib() -> ctypes.CDLL:
     L.hm_snapshot_save.argtypes = [P, C]
     L.hm_snapshot_load.argtypes = [C, ctypes.POINTER(Config), PT]
     L.hm_delete_batch.argtypes = [P, P, SZ, ctypes.POINTER(SZ), P]
+    L.hm_search_baseline.argtypes = [P, I, P, SZ, P, P]
     _lib = L
     return L
 

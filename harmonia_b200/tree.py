@@ -159,6 +159,17 @@ class BPlusTree:
             check(lib().hm_search(self._h, _ptr(keys), n, _ptr(out), _stream_ptr(stream)), "hm_search")
         return out
 
+    def search_pointer_baseline(self, keys, out=None, stream=None):
+        """The HB+-style pointer-chasing comparison kernel (device buffers);
+        same results as search()."""
+        n = len(keys)
+        if out is None:
+            out = _empty_like(keys, n)
+        if n:
+            check(lib().hm_search_baseline(self._h, 1, _ptr(keys), n, _ptr(out), _stream_ptr(stream)),
+                  "hm_search_baseline")
+        return out
+
     def search_batches(self, batches, stream=None) -> None:
         """batches: list of (queries, out) CUDA tensors, searched in one launch."""
         arr = (native.Batch * max(len(batches), 1))()

@@ -294,6 +294,16 @@ int hm_profile(hm_tree *t, int enable);
  * sets *n, and clears the record. */
 int hm_profile_read(hm_tree *t, hm_stage_time *out, int cap, int *n);
 
+/* Comparison kernels for reports, not the product path.  HM_BASELINE_POINTER:
+ * a pointer-chasing descent in the style of the reference's HB+ GPU search
+ * (open-harmonia/src/gbpt.cu:30-113): every inner node stores its children's
+ * ids and each query follows them (one dependent load per level, one thread
+ * per query, no prefix-sum child array, no pre-sort).  Device buffers; the
+ * child-id array (4 B per child slot) is built on the first call after a
+ * rebuild.  Results equal hm_search's. */
+#define HM_BASELINE_POINTER 1
+int hm_search_baseline(hm_tree *t, int kind, const int64_t *q, size_t n, int64_t *out, hm_stream s);
+
 /* ---- Reference dataset files and tree snapshots ------------------------- */
 
 /* Reads a key file in the reference's text format: one signed decimal key per

@@ -273,3 +273,20 @@ def test_bucket_join_after_upserts(c1):
         q = np.concatenate([bk, dg.gen_point_queries(ek, 1 << 20, 0.8, seed=92)])
         t.set_search_config(join=1)
         assert (t.search(cuda(q)).cpu().numpy() == po.PortTree(ek, ev).search(q)).all()
+
+
+@pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (128, 64)])
+def test_pointer_baseline_matches(fanout, leaf_cap):
+    # the HB+-style comparison kernel answers like the product path, also
+    # after a rebuild has replaced the arena
+    keys = dg.gen_keys(1 << 18, 71)
+    sk = np.sort(keys)
+    with BPlusTree.bulk_load(keys, dg.values_for(keys), fanout=fanout, leaf_cap=leaf_cap) as t:
+        q = dg.gen_point_queries(keys, 1 << 17, 0.7, seed=72)
+        q[:3] = [2**63 - 1, -(2**63), sk[0]]
+        dq = cuda(q)
+        assert (t.search_pointer_baseline(dq).cpu().numpy() == po.PortTree(sk, dg.values_for(sk)).search(q)).all()
+        bk, bv = dg.gen_upserts(keys, 60000, 0.9, seed=73)  # full leaves: a rebuild
+        t.upsert(bk, bv)
+        ek, ev = po.upsert_set(sk, dg.values_for(sk), bk, bv)
+        assert (t.search_pointer_baseline(dq).cpu().numpy() == po.PortTree(ek, ev).search(q)).all()
