@@ -134,7 +134,7 @@ int capture(hm_plan *p) {
   // the tile prefix depends on the search parameters: rebuild and upload it
   int rc0 = build_set(t, p->batches.data(), p->nb, p->img, &p->total, &p->tiles);
   if (rc0) return rc0;
-  p->plan = plan_search(t, p->total);
+  p->plan = plan_search(t, p->total, p->nb);
   const size_t need = p->img.size() + batches_work_bytes(t, p->total, p->plan);
   if (need > p->dev_bytes) {  // a retune may need more work memory
     if (p->dev) cudaFree(p->dev);
@@ -199,7 +199,7 @@ int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream hs)
   int64_t total = 0, tiles = 0;
   int rc = build_set(t, batches, nb, img, &total, &tiles);
   if (rc) return rc;
-  const SearchPlan plan = plan_search(t, total);
+  const SearchPlan plan = plan_search(t, total, nb);
   const size_t set_bytes = img.size();
   rc = ensure_scratch(t, set_bytes + batches_work_bytes(t, total, plan));
   if (rc) return rc;

@@ -211,8 +211,9 @@ size_t search_scratch_need(const hm_tree *t, int64_t n) { return plan_search(t, 
 
 namespace hm {
 
-SearchPlan plan_search(const hm_tree *t, int64_t n) {
+SearchPlan plan_search(const hm_tree *t, int64_t n, int batches) {
   SearchPlan p;
+  p.batches = std::max(batches, 1);
   if (n <= 0 || n > INT32_MAX) return p;  // positions are carried as int32
   const hm_config &c = t->cfg;
   const bool join = (c.join == 1 && (c.leaf_cap == 16 || c.leaf_cap == 64)) ||
@@ -226,7 +227,7 @@ SearchPlan plan_search(const hm_tree *t, int64_t n) {
     p.bits = c.sort_bits > 0 ? c.sort_bits : 0;
   }
   if (p.bits > 0) {  // grouped queries, grouped results, partition (offset mode), join
-    p.scratch = 2 * (size_t)align_up(n * 8, 256) + partition_scratch_bytes(n, p.bits, true);
+    p.scratch = 2 * (size_t)align_up(n * 8, 256) + partition_scratch_bytes(n, p.bits, true, p.batches);
     if (p.join) p.scratch += join_scratch_bytes(n, p.bits);
   }
   return p;
@@ -254,7 +255,7 @@ int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int6
   if (rc) return rc;
   tok = prof_begin(t, s);
   if (p.join) {
-    rc = launch_join(t, qs, bstart, p.bits, n, res, ps + partition_scratch_bytes(n, p.bits, true), s);
+    rc = launch_join(t, qs, bstart, p.bits, n, res, ps + partition_scratch_bytes(n, p.bits, true, p.batches), s);
     prof_end(t, kStageJoin, tok, s);
   } else {
     SearchLaunch l{qs, res, nullptr, n};

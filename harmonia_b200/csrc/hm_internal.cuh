@@ -211,7 +211,7 @@ struct BatchView {
 
 // offsets: the partition keeps chunk offsets in the scratch for
 // unpermute_results (pos_out == nullptr); else it writes input positions.
-size_t partition_scratch_bytes(int64_t n, int bits, bool offsets);
+size_t partition_scratch_bytes(int64_t n, int bits, bool offsets, int batches = 1);  // batches: of a batch set
 // Groups queries by the top `bits` bits of their key (relative to the tree's
 // key range); *bucket_start (if given) receives a device pointer, inside the
 // scratch, to the 2^bits + 1 bucket starts.  pos_out: original position of
@@ -266,9 +266,10 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
 struct SearchPlan {
   int bits = 0;
   bool join = false;
+  int batches = 1;  // batches of a batch set (its first pre-sort pass cuts each batch apart)
   size_t scratch = 0;
 };
-SearchPlan plan_search(const hm_tree *t, int64_t n);
+SearchPlan plan_search(const hm_tree *t, int64_t n, int batches = 1);
 int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int64_t n, int64_t *d_out,
                        cudaStream_t s, void *scratch, const BatchView *bv = nullptr);
 

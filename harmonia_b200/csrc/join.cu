@@ -29,7 +29,10 @@ namespace hm {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kPerThread = 4;
+#ifndef HM_JOIN_PER_THREAD
+#define HM_JOIN_PER_THREAD 2  // queries a thread answers per step (measured: 2 beats 4 and 8)
+#endif
+constexpr int kPerThread = HM_JOIN_PER_THREAD;
 constexpr int kRun = kThreads * kPerThread;  // queries a CTA answers per step
 constexpr int kItemRuns = 16;
 constexpr int kItemMax = kRun * kItemRuns;  // queries per work item, at most

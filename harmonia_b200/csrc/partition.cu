@@ -91,80 +91,79 @@ __device__ __forceinline__ int64_t count_index(const Chunk &c, int d) {
   return (int64_t)c.base * 256 + (int64_t)d * c.nchunks + c.idx;
 }
 
-// Reads and writes of a chunk [begin, end) of a flat array, or of the
-// concatenation of a batch set.  One thread resolves the chunk's batches; a
-// chunk inside one batch then goes through a single base pointer, others find
-// each element's batch among the chunk's few.
+// For a batch set, the first pass cuts each batch into its own chunks (a chunk
+// never straddles two batches), numbered globally as one bucket's chunks, so
+// the counts stay laid out [digit][chunk] and the output is one partition of
+// the whole set.  Each chunk carries its batch's pointers shifted by the
+// batch's start: element i of the set is qbase[i] (queries), obase[i]
+// (results).
 struct ChunkIO {
-  int64_t shift;  // base = batch pointer - qpre[batch] when the chunk lies in one batch
-  int b_lo, b_hi;
+  const int64_t *qbase;
+  int64_t *obase;
 };
 
-__device__ __forceinline__ int find_batch(const int64_t *__restrict__ pre, int lo, int hi, int64_t x) {
-  while (lo < hi) {  // last b in [lo, hi] with pre[b] <= x
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(pre + mid) <= x) {
-      lo = mid;
-    } else {
-      hi = mid - 1;
-    }
+// One CTA: the batch set's first-pass chunks and their ChunkIO.
+__global__ void __launch_bounds__(1024) batch_chunk_kernel(BatchView bv, Chunk *__restrict__ chunks,
+                                                            int32_t *__restrict__ nchunks_total,
+                                                            ChunkIO *__restrict__ cio) {
+  __shared__ int32_t pre[1024];
+  const int tid = threadIdx.x, nb = bv.nb;
+  const int per = (nb + 1023) / 1024;
+  int32_t mine = 0;
+  for (int x = 0; x < per; x++) {
+    const int b = tid * per + x;
+    if (b < nb) mine += (int32_t)((bv.qpre[b + 1] - bv.qpre[b] + kChunk - 1) / kChunk);
   }
-  return lo;
-}
-
-template <bool BATCHED>
-__device__ __forceinline__ void resolve_chunk(const BatchView &bv, int64_t begin, int64_t end, ChunkIO *io) {
-  if constexpr (BATCHED) {
-    if (threadIdx.x == 0) {
-      io->b_lo = find_batch(bv.qpre, 0, bv.nb - 1, begin);
-      io->b_hi = find_batch(bv.qpre, io->b_lo, bv.nb - 1, end - 1);
-      io->shift = __ldg(bv.qpre + io->b_lo);
-    }
+  pre[tid] = mine;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan
+    const int32_t v = tid >= o ? pre[tid - o] : 0;
+    __syncthreads();
+    pre[tid] += v;
     __syncthreads();
   }
-}
-
-template <bool BATCHED>
-__device__ __forceinline__ int64_t read_query(const int64_t *__restrict__ q, const BatchView &bv, const ChunkIO &io,
-                                              int64_t i) {
-  if constexpr (!BATCHED) {
-    return __ldg(q + i);
-  } else {
-    const int b = io.b_lo == io.b_hi ? io.b_lo : find_batch(bv.qpre, io.b_lo, io.b_hi, i);
-    const int64_t at = b == io.b_lo ? io.shift : __ldg(bv.qpre + b);
-    return __ldg(bv.batches[b].q + (i - at));
+  const int32_t total = pre[1023];
+  int32_t at = pre[tid] - mine;
+  for (int x = 0; x < per; x++) {
+    const int b = tid * per + x;
+    if (b >= nb) break;
+    const int64_t s = bv.qpre[b], e = bv.qpre[b + 1];
+    const hm_batch bt = bv.batches[b];
+    for (int64_t c0 = s; c0 < e; c0 += kChunk, at++) {
+      Chunk c;
+      c.begin = c0;
+      c.end = min(e, c0 + kChunk);
+      c.bucket = 0;
+      c.idx = at;
+      c.nchunks = total;
+      c.base = 0;
+      chunks[at] = c;
+      ChunkIO io;
+      io.qbase = bt.q - s;  // only indexed inside the batch
+      io.obase = bt.out - s;
+      cio[at] = io;
+    }
   }
+  if (tid == 1023) *nchunks_total = total;
 }
 
 template <bool BATCHED>
-__device__ __forceinline__ void write_result(int64_t *__restrict__ out, const BatchView &bv, const ChunkIO &io,
-                                             int64_t i, int64_t v) {
-  if constexpr (!BATCHED) {
-    out[i] = v;
-  } else {
-    const int b = io.b_lo == io.b_hi ? io.b_lo : find_batch(bv.qpre, io.b_lo, io.b_hi, i);
-    const int64_t at = b == io.b_lo ? io.shift : __ldg(bv.qpre + b);
-    bv.batches[b].out[i - at] = v;
-  }
-}
-
-template <bool BATCHED>
-__global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__restrict__ q, BatchView bv, const Chunk *__restrict__ chunks,
+__global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__restrict__ q, BatchView bv, const ChunkIO *__restrict__ cio,
+                                                        const Chunk *__restrict__ chunks,
                                                         const int32_t *__restrict__ nchunks_total, Bucket bk,
                                                         int shift2, int mask2, int64_t *__restrict__ counts) {
   __shared__ unsigned hist[256];
-  __shared__ ChunkIO io;
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
+  const int64_t *src = BATCHED ? cio[blockIdx.x].qbase : q;  // a chunk lies inside one batch
   for (int i = threadIdx.x; i < 256; i += kThreads) hist[i] = 0;
-  resolve_chunk<BATCHED>(bv, c.begin, c.end, &io);
   __syncthreads();
   for (int64_t base = c.begin; base < c.end; base += 8 * kThreads) {
     int64_t k[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) {  // all loads first
       const int64_t i = base + j * kThreads + threadIdx.x;
-      k[j] = i < c.end ? read_query<BATCHED>(q, bv, io, i) : 0;
+      k[j] = i < c.end ? __ldg(src + i) : 0;
     }
 #pragma unroll
     for (int j = 0; j < 8; j++)
@@ -194,7 +193,8 @@ constexpr int stage_bytes() {
 }
 
 template <typename T, bool LOAD, bool BATCHED>
-__global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(const int64_t *__restrict__ q, BatchView bv, const T *__restrict__ pay_in,
+__global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(const int64_t *__restrict__ q, BatchView bv, const ChunkIO *__restrict__ cio,
+                                                           const T *__restrict__ pay_in,
                                                            const Chunk *__restrict__ chunks,
                                                            const int32_t *__restrict__ nchunks_total, Bucket bk,
                                                            int shift2, int mask2, const int64_t *__restrict__ offs,
@@ -205,22 +205,24 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(c
   __shared__ int64_t gcur[256];
   __shared__ int64_t adj[256];
   __shared__ unsigned wsum[8];
-  __shared__ ChunkIO io;
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const bool digit_thread = tid < 256;  // threads 0..255 own a digit's counters
   if (digit_thread) gcur[tid] = tid <= mask2 ? offs[count_index(c, tid)] : 0;
-  resolve_chunk<BATCHED>(bv, c.begin, c.end, &io);
   int64_t k[kPer];
   T p[kPer];
+  const int64_t *src = BATCHED ? cio[blockIdx.x].qbase : q;  // a chunk lies inside one batch
   auto load_tile = [&](int64_t t0) {
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
       const int64_t i = t0 + j * kSc + tid;
-      const bool valid = i < c.end;
-      k[j] = valid ? read_query<BATCHED>(q, bv, io, i) : 0;
-      p[j] = valid ? payload_of<T, LOAD>(pay_in, c, i) : (T)0;
+      k[j] = i < c.end ? __ldg(src + i) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      const int64_t i = t0 + j * kSc + tid;
+      p[j] = i < c.end ? payload_of<T, LOAD>(pay_in, c, i) : (T)0;
     }
   };
   load_tile(c.begin);
@@ -301,19 +303,18 @@ template <bool BATCHED>
 __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_kernel(
     const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total, const int64_t *__restrict__ offs,
     int nd, const int64_t *__restrict__ res_in, const uint16_t *__restrict__ loc, int64_t *__restrict__ res_out,
-    BatchView bv) {
+    BatchView bv, const ChunkIO *__restrict__ cio) {
   extern __shared__ __align__(16) int64_t staged[];  // kChunk results
   __shared__ int64_t rs[256];
   __shared__ int32_t rl[256];
   __shared__ int32_t up[257];  // first unit of each run
   __shared__ uint8_t unit_run[kChunk / kUnit + 256];
   __shared__ int32_t wsum[8];
-  __shared__ ChunkIO io;
   if ((int)blockIdx.x >= *nchunks_total) return;
   const Chunk c = chunks[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int len = (int)(c.end - c.begin);
-  resolve_chunk<BATCHED>(bv, c.begin, c.end, &io);
+  int64_t *dst = BATCHED ? cio[blockIdx.x].obase : res_out;  // a chunk lies inside one batch
   if (tid < 256) {  // run of digit tid: start, length, units; exclusive scan of the units
     int32_t u = 0;
     if (tid < nd) {
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_ke
         if (lane + 32 * h < cnt[x]) staged[l[x][h]] = r[x][h];
   }
   __syncthreads();
-  for (int x = tid; x < len; x += kRevThreads) write_result<BATCHED>(res_out, bv, io, c.begin + x, staged[x]);
+  for (int x = tid; x < len; x += kRevThreads) dst[c.begin + x] = staged[x];
 }
 
 // One CTA: chunk descriptors for a pass.  bstart == nullptr: the whole input
@@ -491,11 +492,12 @@ struct Work {
   int64_t *q_tmp;    // first-pass keys (two passes); the inverse's temporary
   void *pay1;        // first-pass payloads (two passes)
   uint16_t *loc;     // final offsets (offset mode)
+  ChunkIO *cio;      // batch sets: the batches of each first-pass chunk
 };
 
-size_t work_layout(int64_t n, int bits, bool offsets, Work *w, char *base) {
+size_t work_layout(int64_t n, int bits, bool offsets, Work *w, char *base, int batches = 1) {
   const bool two = bits > 8;
-  const int64_t mc1 = max_chunks(n, 1), mc2 = two ? max_chunks(n, 256) : 0;
+  const int64_t mc1 = max_chunks(n, batches), mc2 = two ? max_chunks(n, 256) : 0;
   const size_t pay = offsets ? 2 : 4;
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -520,6 +522,7 @@ size_t work_layout(int64_t n, int bits, bool offsets, Work *w, char *base) {
   x.q_tmp = two ? reinterpret_cast<int64_t *>(take(8 * n)) : nullptr;
   x.pay1 = two ? take(pay * n) : nullptr;
   x.loc = offsets ? reinterpret_cast<uint16_t *>(take(2 * n)) : nullptr;
+  x.cio = reinterpret_cast<ChunkIO *>(take(sizeof(ChunkIO) * mc1));
   if (w) *w = x;
   return off;
 }
@@ -527,11 +530,14 @@ size_t work_layout(int64_t n, int bits, bool offsets, Work *w, char *base) {
 template <typename T, bool LOAD, bool BATCHED = false>
 void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, const int64_t *bstart_in, int nb,
               int shift2, int mask2, int64_t *q_out, T *pay_out, int64_t *bstart_out, const Pass &ps, void *scan,
-              cudaStream_t s, const BatchView &bv = BatchView()) {
-  chunk_kernel<<<1, 1024, 0, s>>>(bstart_in, nb, n, ps.chunks, ps.nchunks);
+              cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
+  if (BATCHED)
+    batch_chunk_kernel<<<1, 1024, 0, s>>>(bv, ps.chunks, ps.nchunks, const_cast<ChunkIO *>(cio));
+  else
+    chunk_kernel<<<1, 1024, 0, s>>>(bstart_in, nb, n, ps.chunks, ps.nchunks);
   cudaMemsetAsync(ps.offs, 0, sizeof(int64_t) * (256 * ps.mc + 1), s);
-  psa_hist_kernel<BATCHED><<<(unsigned)ps.mc, kThreads, 0, s>>>(q, bv, ps.chunks, ps.nchunks, bk, shift2, mask2,
-                                                                 ps.offs);
+  psa_hist_kernel<BATCHED><<<(unsigned)ps.mc, kThreads, 0, s>>>(q, bv, cio, ps.chunks, ps.nchunks, bk, shift2,
+                                                                 mask2, ps.offs);
   exclusive_scan_i64(ps.offs, ps.offs, 256 * ps.mc, scan, s);
   static bool attr_set = false;  // opt in to > 48 KiB of shared memory once
   if (!attr_set) {
@@ -541,7 +547,7 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
     attr_set = true;
   }
   psa_scatter_kernel<T, LOAD, BATCHED><<<(unsigned)ps.mc, kSc, stage_bytes<T>(), s>>>(
-      q, bv, pay_in, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs, q_out, pay_out);
+      q, bv, cio, pay_in, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs, q_out, pay_out);
   const int nd = mask2 + 1;
   bucket_starts_kernel<<<(unsigned)((nb * nd + 256) / 256), 256, 0, s>>>(ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
                                                                          bstart_in, bstart_out);
@@ -550,7 +556,7 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
 
 template <bool BATCHED = false>
 void unpermute_pass(const Pass &ps, int nd, const int64_t *res_in, const uint16_t *loc, int64_t *res_out,
-                    cudaStream_t s, const BatchView &bv = BatchView()) {
+                    cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(psa_unpermute_kernel<BATCHED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -559,14 +565,14 @@ void unpermute_pass(const Pass &ps, int nd, const int64_t *res_in, const uint16_
     attr_set = true;
   }
   psa_unpermute_kernel<BATCHED><<<(unsigned)ps.mc, kRevThreads, 8 * kChunk, s>>>(ps.chunks, ps.nchunks, ps.offs, nd,
-                                                                                 res_in, loc, res_out, bv);
+                                                                                 res_in, loc, res_out, bv, cio);
   note_launch();
 }
 
 }  // namespace
 
-size_t partition_scratch_bytes(int64_t n, int bits, bool offsets) {
-  return work_layout(n, bits, offsets, nullptr, nullptr) + 256;
+size_t partition_scratch_bytes(int64_t n, int bits, bool offsets, int batches) {
+  return work_layout(n, bits, offsets, nullptr, nullptr, batches) + 256;
 }
 
 int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, int64_t *q_out, int32_t *pos_out,
@@ -576,12 +582,12 @@ int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, i
   const bool offsets = pos_out == nullptr;
   if (bv && !offsets) return HM_EINVAL;
   Work w;
-  work_layout(n, bits, offsets, &w, static_cast<char *>(scratch));
+  work_layout(n, bits, offsets, &w, static_cast<char *>(scratch), bv ? bv->nb : 1);
   const Bucket bk = make_bucket(t, bits);
   if (bits <= 8) {
     if (bv)
       one_pass<uint16_t, false, true>(bk, nullptr, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, w.loc,
-                                      w.bstart, w.p1, w.scan, s, *bv);
+                                      w.bstart, w.p1, w.scan, s, *bv, w.cio);
     else if (offsets)
       one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, w.loc, w.bstart, w.p1,
                                 w.scan, s);
@@ -594,7 +600,7 @@ int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, i
       uint16_t *loc1 = static_cast<uint16_t *>(w.pay1);
       if (bv)
         one_pass<uint16_t, false, true>(bk, nullptr, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1,
-                                        w.p1, w.scan, s, *bv);
+                                        w.p1, w.scan, s, *bv, w.cio);
       else
         one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1, w.p1, w.scan,
                                   s);
@@ -616,7 +622,7 @@ int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, vo
   if (n == 0) return HM_OK;
   if (bits < 1 || bits > 16 || n > INT32_MAX || n < 0) return HM_EINVAL;
   Work w;
-  work_layout(n, bits, true, &w, static_cast<char *>(scratch));
+  work_layout(n, bits, true, &w, static_cast<char *>(scratch), bv ? bv->nb : 1);
   const int64_t *res1 = res_sorted;  // results in first-pass order
   const uint16_t *loc1 = w.loc;
   if (bits > 8) {
@@ -626,7 +632,7 @@ int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, vo
   }
   const int nd1 = bits <= 8 ? 1 << bits : 256;
   if (bv)
-    unpermute_pass<true>(w.p1, nd1, res1, loc1, nullptr, s, *bv);
+    unpermute_pass<true>(w.p1, nd1, res1, loc1, nullptr, s, *bv, w.cio);
   else
     unpermute_pass(w.p1, nd1, res1, loc1, out, s);
   return cuda_err(cudaGetLastError());
