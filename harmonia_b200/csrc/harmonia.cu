@@ -7,6 +7,9 @@
 #include "hm_internal.cuh"
 
 #include <algorithm>
+#include <mutex>
+#include <set>
+#include <tuple>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -267,6 +270,21 @@ int run_planned_search(hm_tree *t, const SearchPlan &p, const int64_t *d_q, int6
   rc = unpermute_results(n, p.bits, res, d_out, ps, s, bv);
   prof_end(t, kStageUnpermute, tok, s);
   return rc;
+}
+
+int opt_in_smem(const void *fn, int bytes) {
+  static std::mutex mu;
+  static std::set<std::tuple<const void *, int, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_err(e);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({fn, dev, bytes})) return HM_OK;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return cuda_err(e);
+  done.insert({fn, dev, bytes});
+  return HM_OK;
 }
 
 // Entry points into this file's helpers for the other host sources.

@@ -259,6 +259,11 @@ size_t join_scratch_bytes(int64_t n, int bits);
 int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int bits,
                 int64_t n, int64_t *out, void *scratch, cudaStream_t s);
 
+// Opts kernel fn in to `bytes` of dynamic shared memory (and the largest
+// shared-memory carveout) on the current device; once per device, kernel and
+// size, from any thread.
+int opt_in_smem(const void *fn, int bytes);
+
 // ---- search plan (harmonia.cu) ----
 // How a batch of n queries is searched: NTG descent on the batch as given
 // (bits = 0), after a pre-sort (bits > 0, join = false), or pre-sort +

@@ -322,14 +322,9 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
   const size_t smem = (size_t)kStages * ml * leaf_bytes(lc);
   const int per_sm = std::max(1, std::min(8, (int)((227 * 1024) / (smem + 1024))));
   const unsigned grid = (unsigned)std::min<int64_t>(max_items(n, nb), (int64_t)t->num_sms * per_sm);
-  static bool attr_set = false;  // opt in to > 48 KiB of shared memory once
-  if (!attr_set) {
-    cudaFuncSetAttribute(join_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStages * kStageMax);
-    cudaFuncSetAttribute(join_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStages * kStageMax);
-    cudaFuncSetAttribute(join_kernel<16>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    cudaFuncSetAttribute(join_kernel<64>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    attr_set = true;
-  }
+  int rc = opt_in_smem(lc == 16 ? (const void *)join_kernel<16> : (const void *)join_kernel<64>,
+                       kStages * kStageMax);
+  if (rc) return rc;
   if (lc == 16) {
     join_kernel<16><<<grid, kThreads, smem, s>>>(t->view(), t->cfg.fanout, items, first + nb, qs, out, ml);
   } else if (lc == 64) {

@@ -539,13 +539,7 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
   psa_hist_kernel<BATCHED><<<(unsigned)ps.mc, kThreads, 0, s>>>(q, bv, cio, ps.chunks, ps.nchunks, bk, shift2,
                                                                  mask2, ps.offs);
   exclusive_scan_i64(ps.offs, ps.offs, 256 * ps.mc, scan, s);
-  static bool attr_set = false;  // opt in to > 48 KiB of shared memory once
-  if (!attr_set) {
-    cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD, BATCHED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         stage_bytes<T>());
-    cudaFuncSetAttribute(psa_scatter_kernel<T, LOAD, BATCHED>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    attr_set = true;
-  }
+  opt_in_smem((const void *)psa_scatter_kernel<T, LOAD, BATCHED>, stage_bytes<T>());
   psa_scatter_kernel<T, LOAD, BATCHED><<<(unsigned)ps.mc, kSc, stage_bytes<T>(), s>>>(
       q, bv, cio, pay_in, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs, q_out, pay_out);
   const int nd = mask2 + 1;
@@ -557,13 +551,7 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
 template <bool BATCHED = false>
 void unpermute_pass(const Pass &ps, int nd, const int64_t *res_in, const uint16_t *loc, int64_t *res_out,
                     cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(psa_unpermute_kernel<BATCHED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(8 * kChunk));
-    cudaFuncSetAttribute(psa_unpermute_kernel<BATCHED>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    attr_set = true;
-  }
+  opt_in_smem((const void *)psa_unpermute_kernel<BATCHED>, (int)(8 * kChunk));
   psa_unpermute_kernel<BATCHED><<<(unsigned)ps.mc, kRevThreads, 8 * kChunk, s>>>(ps.chunks, ps.nchunks, ps.offs, nd,
                                                                                  res_in, loc, res_out, bv, cio);
   note_launch();

@@ -343,19 +343,20 @@ KernelFn pick_kernel(int w, int f, int lc, int qpg) {
 struct GridCache {
   KernelFn fn = nullptr;
   size_t smem = 0;
+  int device = 0;
   int blocks_per_sm = 0;
 };
 
 int grid_for(const hm_tree *t, KernelFn fn, size_t smem, int *blocks) {
   static thread_local GridCache cache[8];
   for (auto &c : cache)
-    if (c.fn == fn && c.smem == smem) {
+    if (c.fn == fn && c.smem == smem && c.device == t->device) {
       *blocks = c.blocks_per_sm * t->num_sms;
       return HM_OK;
     }
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_err(e);
+    int rc = opt_in_smem((const void *)fn, (int)smem);
+    if (rc) return rc;
   }
   int per = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kThreads, smem);
@@ -364,6 +365,7 @@ int grid_for(const hm_tree *t, KernelFn fn, size_t smem, int *blocks) {
   for (auto &c : cache)
     if (c.fn == nullptr) {
       c.fn = fn;
+      c.device = t->device;
       c.smem = smem;
       c.blocks_per_sm = per;
       break;

@@ -664,13 +664,8 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     note_launch();
     if (hf & 1u) {
       const size_t smem = (size_t)t->cfg.fanout * lc * sizeof(longlong2);
-      static bool attr_set = false;  // up to 128 KiB (fanout 128, 64-key leaves)
-      if (!attr_set) {
-        e = cudaFuncSetAttribute(subtree_rebalance_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 128 * 64 * (int)sizeof(longlong2));
-        if (e != cudaSuccess) return cuda_err(e);
-        attr_set = true;
-      }
+      rc = opt_in_smem((const void *)subtree_rebalance_kernel, 128 * 64 * (int)sizeof(longlong2));  // up to 128 KiB
+      if (rc) return rc;
       subtree_rebalance_kernel<<<(unsigned)last_nodes, kThreads, smem, s>>>(
           t->inner, t->prefix, t->leaf_rows, t->leaf_cnt, t->leaf_base, t->cfg.fanout, lc, li, g, mark, mk, mv, ml,
           nm);
