@@ -272,10 +272,13 @@ int stage_leaves_for(const hm_tree *t, int bits) {
 
 }  // namespace
 
+#ifndef HM_JOIN_MAX_BITS
+#define HM_JOIN_MAX_BITS 16
+#endif
 int join_bits(const hm_tree *t) {
-  // 16 bits, or fewer while buckets still average at most 32 leaves
+  // HM_JOIN_MAX_BITS bits, or fewer while buckets still average at most 32 leaves
   int b = 1;
-  while (b < 16 && (t->n_leaf >> b) > 32) b++;
+  while (b < HM_JOIN_MAX_BITS && (t->n_leaf >> b) > 32) b++;
   return b;
 }
 

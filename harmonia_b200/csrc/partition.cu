@@ -17,8 +17,8 @@
 //     second pass partitions every first-pass bucket on its own, in chunks that
 //     never straddle a bucket, with offsets from one global scan of counts laid
 //     out as [bucket][digit][chunk];
-//   * each pass stages a 4096-query tile in shared memory grouped by digit
-//     (one 16-B slot per query: key, digit and payload) and writes it out so
+//   * each pass stages an 8192-query tile in shared memory grouped by digit
+//     (12 B per query: key, digit and position) and writes it out so
 //     consecutive threads store consecutive slots;
 //   * the payload is either the query's input position (int32, for callers
 //     that scatter results themselves) or its offset inside its 8192-query
@@ -36,22 +36,13 @@ namespace hm {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int64_t kChunk = 8192;  // queries per CTA chunk (offsets inside a chunk fit 16 bits)
 #ifndef HM_PSA_TILE
-#define HM_PSA_TILE 4096  // queries a scatter CTA stages at a time
+#define HM_PSA_TILE 8192  // queries a scatter CTA stages at a time (a divisor of kChunk)
 #endif
 constexpr int kTile = HM_PSA_TILE;
-constexpr int64_t kChunk = 8192;  // queries per CTA chunk (a multiple of kTile; offsets fit 16 bits)
 
 // Launch shapes (compile-time tunables, measured on B200 at 2^24 queries).
-#ifndef HM_PSA_SCATTER_THREADS
-#define HM_PSA_SCATTER_THREADS 256  // threads of a scatter CTA (256, 512 or 1024)
-#endif
-#ifndef HM_PSA_SCATTER_MINB
-#define HM_PSA_SCATTER_MINB 3  // resident scatter CTAs per SM the register budget allows
-#endif
-constexpr int kSc = HM_PSA_SCATTER_THREADS;
-constexpr int kPer = kTile / kSc;
-static_assert(kSc >= 256 && kTile % kSc == 0 && kTile <= 65536, "a thread per digit; ranks kept in 16 bits");
 #ifndef HM_PSA_REV_THREADS
 #define HM_PSA_REV_THREADS 512
 #endif
@@ -144,7 +135,10 @@ __global__ void __launch_bounds__(1024) batch_chunk_kernel(BatchView bv, Chunk *
       cio[at] = io;
     }
   }
-  if (tid == 1023) *nchunks_total = total;
+  if (tid == 1023) {
+    nchunks_total[0] = total;
+    nchunks_total[1] = 0;  // work counter of the persistent scatter
+  }
 }
 
 template <bool BATCHED>
@@ -173,66 +167,68 @@ __global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__res
   for (int d = threadIdx.x; d <= mask2; d += kThreads) counts[count_index(c, d)] = hist[d];
 }
 
-// Payload of the element at input position i of chunk c: loaded from pay_in
-// (LOAD), else generated: the position i (int32) or its offset i - c.begin
-// inside the chunk (uint16).
-template <typename T, bool LOAD>
-__device__ __forceinline__ T payload_of(const T *__restrict__ pay_in, const Chunk &c, int64_t i) {
-  if constexpr (LOAD) {
-    return __ldg(pay_in + i);
-  } else if constexpr (sizeof(T) == 2) {
-    return (T)(i - c.begin);
-  } else {
-    return (T)i;
-  }
-}
-
-template <typename T>
-constexpr int stage_bytes() {
-  return kTile * 16;  // one 16-B slot per staged element: key, then digit << 32 | payload
-}
+// Scatter of one pass.  A grid of resident CTAs takes chunks from a counter
+// (the first one by block index).  Per tile: rank every query inside its
+// digit with shared-memory atomics, scan the 256 tile counts, stage the tile
+// grouped by digit as keys (8 B) plus an aux word (digit << 16 | position in
+// the tile), then write it out so consecutive threads store consecutive slots
+// of one digit run.  The loads of the next tile -- the next chunk's first tile
+// at a chunk's end -- are issued before the write-out.  The payload is derived
+// from the position at write-out: the input position (int32), the offset
+// inside the chunk (uint16), or loaded from pay_in (LOAD).
+#ifndef HM_PSA_SCATTER_THREADS
+#define HM_PSA_SCATTER_THREADS 512
+#endif
+#ifndef HM_PSA_SCATTER_MINB
+#define HM_PSA_SCATTER_MINB 2  // resident CTAs per SM (shared memory holds 2 at 8192-query tiles)
+#endif
+constexpr int kSc = HM_PSA_SCATTER_THREADS;
+constexpr int kPer = kTile / kSc;
+static_assert(kSc >= 256 && kTile % kSc == 0 && kChunk % kTile == 0, "a thread per digit; positions in 16 bits");
+constexpr int stage_bytes() { return kTile * 12; }
 
 template <typename T, bool LOAD, bool BATCHED>
-__global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(const int64_t *__restrict__ q, BatchView bv, const ChunkIO *__restrict__ cio,
-                                                           const T *__restrict__ pay_in,
-                                                           const Chunk *__restrict__ chunks,
-                                                           const int32_t *__restrict__ nchunks_total, Bucket bk,
-                                                           int shift2, int mask2, const int64_t *__restrict__ offs,
-                                                           int64_t *__restrict__ q_out, T *__restrict__ pay_out) {
-  extern __shared__ __align__(16) longlong2 slot[];  // kTile staged elements, dynamic
+__global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(
+    const int64_t *__restrict__ q, const ChunkIO *__restrict__ cio, const T *__restrict__ pay_in,
+    const Chunk *__restrict__ chunks, int32_t *__restrict__ nchunks_total, Bucket bk, int shift2, int mask2,
+    const int64_t *__restrict__ offs, int64_t *__restrict__ q_out, T *__restrict__ pay_out) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  int64_t *skey = reinterpret_cast<int64_t *>(dyn);                 // grouped keys
+  uint32_t *saux = reinterpret_cast<uint32_t *>(dyn + 8 * kTile);  // digit << 16 | tile position
   __shared__ unsigned cnt[256];
   __shared__ unsigned tstart[256];
   __shared__ int64_t gcur[256];
   __shared__ int64_t adj[256];
   __shared__ unsigned wsum[8];
-  if ((int)blockIdx.x >= *nchunks_total) return;
-  const Chunk c = chunks[blockIdx.x];
+  __shared__ int next_chunk;
+  const int nct = nchunks_total[0];
+  int ci = blockIdx.x;
+  if (ci >= nct) return;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const bool digit_thread = tid < 256;  // threads 0..255 own a digit's counters
-  if (digit_thread) gcur[tid] = tid <= mask2 ? offs[count_index(c, tid)] : 0;
+  Chunk c = chunks[ci];
+  const int64_t *src = BATCHED ? cio[ci].qbase : q;  // a chunk lies inside one batch
   int64_t k[kPer];
-  T p[kPer];
-  const int64_t *src = BATCHED ? cio[blockIdx.x].qbase : q;  // a chunk lies inside one batch
-  auto load_tile = [&](int64_t t0) {
+  auto load_tile = [&](const int64_t *sp, int64_t t0, int64_t end) {
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
       const int64_t i = t0 + j * kSc + tid;
-      k[j] = i < c.end ? __ldg(src + i) : 0;
-    }
-#pragma unroll
-    for (int j = 0; j < kPer; j++) {
-      const int64_t i = t0 + j * kSc + tid;
-      p[j] = i < c.end ? payload_of<T, LOAD>(pay_in, c, i) : (T)0;
+      k[j] = i < end ? __ldg(sp + i) : 0;
     }
   };
-  load_tile(c.begin);
-  for (int64_t t0 = c.begin; t0 < c.end; t0 += kTile) {
+  load_tile(src, c.begin, c.end);
+  if (digit_thread) gcur[tid] = tid <= mask2 ? offs[count_index(c, tid)] : 0;
+  int64_t t0 = c.begin;
+  for (;;) {
+    const bool last_tile = t0 + kTile >= c.end;
     if (digit_thread) cnt[tid] = 0;
+    if (tid == 0 && last_tile) next_chunk = (int)gridDim.x + atomicAdd(&nchunks_total[1], 1);
     __syncthreads();
+    const int n = (int)min((int64_t)kTile, c.end - t0);
     unsigned dr[kPer];  // digit << 16 | rank inside the tile's digit run; ~0u past the end
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
-      if (t0 + j * kSc + tid < c.end) {
+      if (j * kSc + tid < n) {
         const unsigned d = (unsigned)((bk(k[j]) >> shift2) & mask2);
         dr[j] = d << 16 | atomicAdd(&cnt[d], 1u);
       } else {
@@ -265,20 +261,48 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(c
       if (dr[j] != ~0u) {
         const unsigned d = dr[j] >> 16;
         const unsigned sl = tstart[d] + (dr[j] & 0xffffu);
-        slot[sl] = make_longlong2(k[j], (long long)((uint64_t)d << 32 | (uint32_t)p[j]));
+        skey[sl] = k[j];
+        saux[sl] = d << 16 | (unsigned)(j * kSc + tid);
       }
     }
     __syncthreads();
-    if (t0 + kTile < c.end) load_tile(t0 + kTile);  // the next tile's loads overlap the write-out
-    const int n = (int)min((int64_t)kTile, c.end - t0);
+    // issue the next tile's loads (this chunk's next tile, or the next chunk's first)
+    const int64_t cur_t0 = t0, cur_off = t0 - c.begin;
+    bool more = true;
+    if (!last_tile) {
+      t0 += kTile;
+      load_tile(src, t0, c.end);
+    } else {
+      ci = next_chunk;
+      more = ci < nct;
+      if (more) {
+        c = chunks[ci];
+        src = BATCHED ? cio[ci].qbase : q;
+        t0 = c.begin;
+        load_tile(src, t0, c.end);
+      }
+    }
     for (int sl = tid; sl < n; sl += kSc) {
-      const longlong2 e = slot[sl];
-      const int64_t o = adj[(uint64_t)e.y >> 32] + sl;
-      q_out[o] = e.x;
-      pay_out[o] = (T)(uint32_t)e.y;
+      const int64_t key = skey[sl];
+      const unsigned a = saux[sl];
+      const int64_t o = adj[a >> 16] + sl;
+      const unsigned e = a & 0xffffu;
+      q_out[o] = key;
+      if constexpr (LOAD)
+        pay_out[o] = __ldg(pay_in + cur_t0 + e);
+      else if constexpr (sizeof(T) == 2)
+        pay_out[o] = (T)(cur_off + e);
+      else
+        pay_out[o] = (T)(cur_t0 + e);
     }
     __syncthreads();
-    if (digit_thread) gcur[tid] += cnt[tid];
+    if (!more) break;
+    if (digit_thread) {
+      if (last_tile)
+        gcur[tid] = tid <= mask2 ? offs[count_index(c, tid)] : 0;
+      else
+        gcur[tid] += cnt[tid];
+    }
   }
 }
 
@@ -397,7 +421,10 @@ __global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__
       c.base = 0;
       chunks[i] = c;
     }
-    if (tid == 0) *nchunks_total = nc;
+    if (tid == 0) {
+      nchunks_total[0] = nc;
+      nchunks_total[1] = 0;  // work counter of the persistent scatter
+    }
     return;
   }
   const int per = (nb + 1023) / 1024;
@@ -432,7 +459,10 @@ __global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__
     }
     base += nc;
   }
-  if (tid == 1023) *nchunks_total = pre[1023];
+  if (tid == 1023) {
+    nchunks_total[0] = pre[1023];
+    nchunks_total[1] = 0;
+  }
 }
 
 // Starts of the pass's output buckets: bucket (b, d) starts at the offset of
@@ -530,7 +560,7 @@ size_t work_layout(int64_t n, int bits, bool offsets, Work *w, char *base, int b
 template <typename T, bool LOAD, bool BATCHED = false>
 void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, const int64_t *bstart_in, int nb,
               int shift2, int mask2, int64_t *q_out, T *pay_out, int64_t *bstart_out, const Pass &ps, void *scan,
-              cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
+              int sms, cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
   if (BATCHED)
     batch_chunk_kernel<<<1, 1024, 0, s>>>(bv, ps.chunks, ps.nchunks, const_cast<ChunkIO *>(cio));
   else
@@ -539,9 +569,10 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
   psa_hist_kernel<BATCHED><<<(unsigned)ps.mc, kThreads, 0, s>>>(q, bv, cio, ps.chunks, ps.nchunks, bk, shift2,
                                                                  mask2, ps.offs);
   exclusive_scan_i64(ps.offs, ps.offs, 256 * ps.mc, scan, s);
-  opt_in_smem((const void *)psa_scatter_kernel<T, LOAD, BATCHED>, stage_bytes<T>());
-  psa_scatter_kernel<T, LOAD, BATCHED><<<(unsigned)ps.mc, kSc, stage_bytes<T>(), s>>>(
-      q, bv, cio, pay_in, ps.chunks, ps.nchunks, bk, shift2, mask2, ps.offs, q_out, pay_out);
+  opt_in_smem((const void *)psa_scatter_kernel<T, LOAD, BATCHED>, stage_bytes());
+  const unsigned grid = (unsigned)std::min<int64_t>(ps.mc, (int64_t)sms * HM_PSA_SCATTER_MINB);
+  psa_scatter_kernel<T, LOAD, BATCHED><<<grid, kSc, stage_bytes(), s>>>(q, cio, pay_in, ps.chunks, ps.nchunks, bk,
+                                                                         shift2, mask2, ps.offs, q_out, pay_out);
   const int nd = mask2 + 1;
   bucket_starts_kernel<<<(unsigned)((nb * nd + 256) / 256), 256, 0, s>>>(ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
                                                                          bstart_in, bstart_out);
@@ -572,33 +603,34 @@ int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, i
   Work w;
   work_layout(n, bits, offsets, &w, static_cast<char *>(scratch), bv ? bv->nb : 1);
   const Bucket bk = make_bucket(t, bits);
+  const int sms = t->num_sms;
   if (bits <= 8) {
     if (bv)
       one_pass<uint16_t, false, true>(bk, nullptr, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, w.loc,
-                                      w.bstart, w.p1, w.scan, s, *bv, w.cio);
+                                      w.bstart, w.p1, w.scan, sms, s, *bv, w.cio);
     else if (offsets)
       one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, w.loc, w.bstart, w.p1,
-                                w.scan, s);
+                                w.scan, sms, s);
     else
       one_pass<int32_t, false>(bk, q, nullptr, n, nullptr, 1, 0, (1 << bits) - 1, q_out, pos_out, w.bstart, w.p1,
-                               w.scan, s);
+                               w.scan, sms, s);
   } else {
     const int low = bits - 8;
     if (offsets) {
       uint16_t *loc1 = static_cast<uint16_t *>(w.pay1);
       if (bv)
         one_pass<uint16_t, false, true>(bk, nullptr, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1,
-                                        w.p1, w.scan, s, *bv, w.cio);
+                                        w.p1, w.scan, sms, s, *bv, w.cio);
       else
         one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1, w.p1, w.scan,
-                                  s);
+                                  sms, s);
       one_pass<uint16_t, false>(bk, w.q_tmp, nullptr, n, w.bstart1, 256, 0, (1 << low) - 1, q_out, w.loc, w.bstart,
-                                w.p2, w.scan, s);
+                                w.p2, w.scan, sms, s);
     } else {
       int32_t *pos1 = static_cast<int32_t *>(w.pay1);
-      one_pass<int32_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, pos1, w.bstart1, w.p1, w.scan, s);
+      one_pass<int32_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, pos1, w.bstart1, w.p1, w.scan, sms, s);
       one_pass<int32_t, true>(bk, w.q_tmp, pos1, n, w.bstart1, 256, 0, (1 << low) - 1, q_out, pos_out, w.bstart, w.p2,
-                              w.scan, s);
+                              w.scan, sms, s);
     }
   }
   if (bucket_start) *bucket_start = w.bstart;
