@@ -89,7 +89,41 @@ using namespace hm;
 
 namespace {
 
-constexpr int64_t kChunk = 1 << 22;  // queries per host-pipeline chunk
+// Chunks of the host-buffer pipeline: the first and last ones small (the
+// first copy in and the last search + copy out run alone), the middle ones
+// large (each chunk costs a few microseconds of copy setup and stream waits).
+#ifndef HM_HOST_CHUNK
+#define HM_HOST_CHUNK (1 << 21)
+#endif
+#ifndef HM_HOST_CHUNK_MIN
+#define HM_HOST_CHUNK_MIN (1 << 18)
+#endif
+constexpr int64_t kChunk = HM_HOST_CHUNK;
+constexpr int64_t kChunkMin = HM_HOST_CHUNK_MIN;
+
+// Chunk sizes for n queries: doubling from kChunkMin up to kChunk, kChunk
+// while the ramp down still fits, then halving back to kChunkMin.
+std::vector<int64_t> chunk_schedule(int64_t n) {
+  std::vector<int64_t> up, down;
+  int64_t left = n;
+  for (int64_t c = kChunkMin; c < kChunk && left > 0; c *= 2) {  // ramp up
+    const int64_t m = std::min(c, left);
+    up.push_back(m);
+    left -= m;
+  }
+  for (int64_t c = kChunkMin; c < kChunk && left > 0; c *= 2) {  // ramp down, built from the end
+    const int64_t m = std::min(c, left);
+    down.push_back(m);
+    left -= m;
+  }
+  while (left > 0) {
+    const int64_t m = std::min(kChunk, left);
+    up.push_back(m);
+    left -= m;
+  }
+  up.insert(up.end(), down.rbegin(), down.rend());
+  return up;
+}
 
 bool is_device_ptr(const void *p) {
   if (!p) return false;
@@ -515,76 +549,85 @@ int hm_search(hm_tree *t, const int64_t *q, size_t n_, int64_t *out, hm_stream h
     return search_device(t, q, n, out, s, t->scratch, t->scratch_bytes);
   }
   if (dq != dout) return HM_EINVAL;  // mixed host/device buffers are not supported
-  // Host buffers: chunked pipeline, copies on two streams overlapping the search.
+  // Host buffers: chunked pipeline over a ring of kIoRing device buffers, copies
+  // in and out on their own streams overlapping the search of other chunks.
   int rc = ensure_io(t);
   if (rc) return rc;
-  const int64_t chunk = std::min<int64_t>(kChunk, n);
+  constexpr int R = kIoRing;
+  const std::vector<int64_t> sizes = chunk_schedule(n);
+  int64_t chunk = 0;
+  size_t sneed = 0;
+  for (int64_t m : sizes) {
+    chunk = std::max(chunk, m);
+    sneed = std::max(sneed, search_scratch_need(t, m));
+  }
   const size_t cbytes = (size_t)align_up(chunk * 8, 256);
-  const size_t sneed = search_scratch_need(t, chunk);
-  rc = ensure_scratch(t, 4 * cbytes + sneed);
+  rc = ensure_scratch(t, 2 * R * cbytes + sneed);
   if (rc) return rc;
   char *sb = static_cast<char *>(t->scratch);
-  int64_t *dqb[2] = {reinterpret_cast<int64_t *>(sb), reinterpret_cast<int64_t *>(sb + cbytes)};
-  int64_t *dob[2] = {reinterpret_cast<int64_t *>(sb + 2 * cbytes),
-                     reinterpret_cast<int64_t *>(sb + 3 * cbytes)};
-  void *search_scratch = sb + 4 * cbytes;
+  int64_t *dqb[R], *dob[R];
+  for (int b = 0; b < R; b++) {
+    dqb[b] = reinterpret_cast<int64_t *>(sb + (size_t)b * cbytes);
+    dob[b] = reinterpret_cast<int64_t *>(sb + (size_t)(R + b) * cbytes);
+  }
+  void *search_scratch = sb + 2 * R * cbytes;
   const bool pinned = is_pinned_host(q) && is_pinned_host(out);
-  int64_t *hq[2] = {nullptr, nullptr}, *ho[2] = {nullptr, nullptr};
+  int64_t *hq[R] = {}, *ho[R] = {};
   if (!pinned) {
-    rc = ensure_pinned(t, 4 * cbytes);
+    rc = ensure_pinned(t, 2 * R * cbytes);
     if (rc) return rc;
     char *pb = static_cast<char *>(t->pinned);
-    hq[0] = reinterpret_cast<int64_t *>(pb);
-    hq[1] = reinterpret_cast<int64_t *>(pb + cbytes);
-    ho[0] = reinterpret_cast<int64_t *>(pb + 2 * cbytes);
-    ho[1] = reinterpret_cast<int64_t *>(pb + 3 * cbytes);
+    for (int b = 0; b < R; b++) {
+      hq[b] = reinterpret_cast<int64_t *>(pb + (size_t)b * cbytes);
+      ho[b] = reinterpret_cast<int64_t *>(pb + (size_t)(R + b) * cbytes);
+    }
   }
   cudaStream_t sin = t->io_stream[0], scomp = t->io_stream[1], sout = t->io_stream[2];
-  cudaEvent_t *ev_in = t->io_event, *ev_comp = t->io_event + 2, *ev_out = t->io_event + 4;
+  cudaEvent_t *ev_in = t->io_event, *ev_comp = t->io_event + R, *ev_out = t->io_event + 2 * R;
+  cudaEvent_t ev_order = t->io_event[3 * R];
   // Order the pipeline after prior work on the caller's stream.
-  cudaEventRecord(t->io_event[6], s);
-  cudaStreamWaitEvent(sin, t->io_event[6], 0);
-  cudaStreamWaitEvent(scomp, t->io_event[6], 0);
-  const int64_t nchunks = (n + chunk - 1) / chunk;
+  cudaEventRecord(ev_order, s);
+  cudaStreamWaitEvent(sin, ev_order, 0);
+  cudaStreamWaitEvent(scomp, ev_order, 0);
+  const int64_t nchunks = (int64_t)sizes.size();
+  std::vector<int64_t> starts(nchunks + 1, 0);
+  for (int64_t c = 0; c < nchunks; c++) starts[c + 1] = starts[c] + sizes[c];
   cudaError_t e = cudaSuccess;
   for (int64_t c = 0; c < nchunks && e == cudaSuccess; c++) {
-    const int b = (int)(c & 1);
-    const int64_t o = c * chunk, m = std::min(chunk, n - o);
-    if (c >= 2) cudaStreamWaitEvent(sin, ev_comp[b], 0);  // dqb[b] no longer read
+    const int b = (int)(c % R);
+    const bool reuse = c >= R;  // ring slot b held chunk c - R
+    const int64_t o = starts[c], m = sizes[c];
+    if (reuse) cudaStreamWaitEvent(sin, ev_comp[b], 0);  // dqb[b] no longer read
     if (pinned) {
       e = cudaMemcpyAsync(dqb[b], q + o, m * 8, cudaMemcpyHostToDevice, sin);
     } else {
-      if (c >= 2) cudaEventSynchronize(ev_in[b]);  // staging hq[b] consumed
+      if (reuse) cudaEventSynchronize(ev_in[b]);  // staging hq[b] consumed
       std::memcpy(hq[b], q + o, m * 8);
       e = cudaMemcpyAsync(dqb[b], hq[b], m * 8, cudaMemcpyHostToDevice, sin);
     }
     cudaEventRecord(ev_in[b], sin);
     cudaStreamWaitEvent(scomp, ev_in[b], 0);
-    if (c >= 2) cudaStreamWaitEvent(scomp, ev_out[b], 0);  // dob[b] drained
+    if (reuse) cudaStreamWaitEvent(scomp, ev_out[b], 0);  // dob[b] drained
     rc = search_device(t, dqb[b], m, dob[b], scomp, search_scratch, sneed);
     if (rc) break;
     cudaEventRecord(ev_comp[b], scomp);
     cudaStreamWaitEvent(sout, ev_comp[b], 0);
     if (pinned) {
       e = cudaMemcpyAsync(out + o, dob[b], m * 8, cudaMemcpyDeviceToHost, sout);
-      cudaEventRecord(ev_out[b], sout);
     } else {
-      if (c >= 2) {
-        // drain chunk c-2 from staging before reusing ho[b]
+      if (reuse) {
+        // drain chunk c - R from staging before reusing ho[b]
         cudaEventSynchronize(ev_out[b]);
-        const int64_t po = (c - 2) * chunk, pm = std::min(chunk, n - po);
-        std::memcpy(out + po, ho[b], pm * 8);
+        std::memcpy(out + starts[c - R], ho[b], sizes[c - R] * 8);
       }
       e = cudaMemcpyAsync(ho[b], dob[b], m * 8, cudaMemcpyDeviceToHost, sout);
-      cudaEventRecord(ev_out[b], sout);
     }
+    cudaEventRecord(ev_out[b], sout);
   }
   if (rc == HM_OK && e == cudaSuccess) e = cudaStreamSynchronize(sout);
   if (rc == HM_OK && e == cudaSuccess && !pinned) {
-    for (int64_t c = std::max<int64_t>(0, nchunks - 2); c < nchunks; c++) {
-      const int b = (int)(c & 1);
-      const int64_t po = c * chunk, pm = std::min(chunk, n - po);
-      std::memcpy(out + po, ho[b], pm * 8);
+    for (int64_t c = std::max<int64_t>(0, nchunks - R); c < nchunks; c++) {
+      std::memcpy(out + starts[c], ho[(int)(c % R)], sizes[c] * 8);
     }
   }
   cudaStreamSynchronize(scomp);

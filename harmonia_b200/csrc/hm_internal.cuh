@@ -35,6 +35,10 @@ namespace hm {
 constexpr int64_t kMaxKey = INT64_MAX;
 constexpr uint64_t kSign = 0x8000000000000000ull;
 constexpr int kMaxLevels = 32;
+#ifndef HM_HOST_RING
+#define HM_HOST_RING 4
+#endif
+constexpr int kIoRing = HM_HOST_RING;  // chunks of the host-buffer pipeline in flight
 
 // Error word bits a kernel may set (read back by hm_sync).
 enum : unsigned {
@@ -131,7 +135,7 @@ struct hm_tree {
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
   cudaStream_t io_stream[3] = {nullptr, nullptr, nullptr};
-  cudaEvent_t io_event[8] = {};
+  cudaEvent_t io_event[3 * hm::kIoRing + 1] = {};  // per ring slot: copied in, searched, copied out; + order
   // stage timing (hm_profile): event pairs recorded around each stage
   struct ProfRec {
     int stage;

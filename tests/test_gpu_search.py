@@ -107,7 +107,7 @@ def test_configs_against_small_golden(fanout, leaf_cap):
 
 def test_host_pageable_and_pinned_buffers(c1):
     keys, sk, t = c1
-    q = dg.gen_point_queries(keys, (1 << 22) * 2 + 12345, 0.5, seed=77)  # > 2 pipeline chunks
+    q = dg.gen_point_queries(keys, (1 << 22) * 2 + 12345, 0.5, seed=77)  # more chunks than the ring holds
     exp = po.PortTree(sk, dg.values_for(sk)).search(q)
     assert (t.search(q) == exp).all()
     qp = torch.from_numpy(q).pin_memory()
