@@ -36,6 +36,7 @@ constexpr int kPerThread = HM_JOIN_PER_THREAD;
 constexpr int kRun = kThreads * kPerThread;  // queries a CTA answers per step
 constexpr int kItemRuns = 16;
 constexpr int kItemMax = kRun * kItemRuns;  // queries per work item, at most
+static_assert(kItemMax < 65536, "an item's query count is kept in 16 bits");
 #ifndef HM_JOIN_STAGES
 #define HM_JOIN_STAGES 2  // shared-memory ring of the join kernel
 #endif
@@ -51,7 +52,10 @@ constexpr int kStageMax = (216 / kStages) * 1024;  // shared memory of one stage
 // A work item: at most kItemMax queries of one bucket and the bucket's leaves
 // [l0, l0 + nl); the leaves are staged once for all of them.
 struct __align__(16) Item {
-  int32_t qa, len, l0, nl;
+  int32_t qa, l0, b;  // first query, first leaf, bucket
+  uint32_t len_nl;    // queries (at most kItemMax) << 16 | leaves (capped at 65535)
+  __host__ __device__ int len() const { return (int)(len_nl >> 16); }
+  __host__ __device__ int nl() const { return (int)(len_nl & 0xffffu); }
 };
 
 // Per bucket b in [0, nb]: leafb[b] = leaf holding the smallest key of bucket
@@ -92,9 +96,10 @@ __global__ void expand_items_kernel(int nb, const int64_t *__restrict__ bstart, 
     for (int r = 0; r < c; r++) {
       Item it;
       it.qa = (int32_t)(s + (int64_t)r * kItemMax);
-      it.len = (int32_t)min((int64_t)kItemMax, e - (s + (int64_t)r * kItemMax));
+      const int32_t len = (int32_t)min((int64_t)kItemMax, e - (s + (int64_t)r * kItemMax));
       it.l0 = l0;
-      it.nl = nl;
+      it.b = b;
+      it.len_nl = (uint32_t)len << 16 | (uint32_t)min(nl, 65535);  // a capped count is never staged
       items[o + r] = it;
     }
   }
@@ -134,9 +139,9 @@ __device__ __forceinline__ void stage_leaves(const DevTree &t, const Item &it, S
   constexpr int LI = LC >= 32 ? LC / 8 : 0;
   constexpr int ROW = LI + 2 * LC;
   constexpr int KS = LC + 1;
-  if (it.nl < 1 || it.nl > ml) return;
+  if (it.nl() < 1 || it.nl() > ml) return;
   const longlong2 *src = reinterpret_cast<const longlong2 *>(t.leaf_rows + (int64_t)it.l0 * ROW);
-  const int nvec = it.nl * (ROW / 2);
+  const int nvec = it.nl() * (ROW / 2);
   for (int v = threadIdx.x; v < nvec; v += kThreads) {
     const int m = v / (ROW / 2), w = 2 * (v - m * (ROW / 2));
     if (w < LI) continue;
@@ -166,6 +171,65 @@ __device__ __forceinline__ int64_t lookup_staged(Stage<LC> st, int nl, int span,
   return kr[c] == q ? st.vp[m * LC + c] : HM_NOT_FOUND;
 }
 
+// Directory of the staged leaves of one item (bucket b): slot j covers the
+// keys [s_j, s_j+1) with s_j = bucket low + j << dshift, and dir[j] is the
+// last leaf whose first key is <= s_j (0 if none), so a query of slot j lies
+// in a leaf of [dir[j], dir[j+1]] (dir[D] = nl - 1).  Keys are compared in the
+// biased unsigned order (k ^ sign bit), which is the signed order.
+#ifndef HM_JOIN_DIR_BITS
+#define HM_JOIN_DIR_BITS 6
+#endif
+constexpr int kDirBits = HM_JOIN_DIR_BITS;
+constexpr int kDir = 1 << kDirBits;
+#ifndef HM_JOIN_DIR_MIN
+#define HM_JOIN_DIR_MIN 768  // mean queries per bucket from which the directory kernel runs
+#endif
+
+__host__ __device__ __forceinline__ uint64_t biased(int64_t k) { return (uint64_t)k ^ kSign; }
+
+template <int LC>
+__device__ __forceinline__ void build_dir(Stage<LC> st, int nl, int span, uint64_t lo_u, int dshift,
+                                          int32_t *dir) {
+  constexpr int KS = LC + 1;
+  for (int j = threadIdx.x; j <= kDir; j += kThreads) {
+    if (j == kDir) {
+      dir[j] = nl - 1;
+      continue;
+    }
+    uint64_t sj = lo_u + ((uint64_t)j << dshift);
+    if (sj < lo_u) sj = ~0ull;  // past the top of the key space
+    int m = 0;
+    for (int step = span >> 1; step > 0; step >>= 1)
+      if (m + step < nl && biased(st.kp[(m + step) * KS]) <= sj) m += step;
+    dir[j] = m;
+  }
+}
+
+template <int LC>
+__device__ __forceinline__ int64_t lookup_dir(Stage<LC> st, int nl, const int32_t *dir, uint64_t lo_u, int dshift,
+                                              int64_t q) {
+  constexpr int KS = LC + 1;
+  const uint64_t qu = biased(q);
+  int m, hi;
+  if (qu < lo_u) {  // below the bucket (bucket 0 only: not a loaded key)
+    m = 0;
+    hi = dir[0];
+  } else {
+    const uint64_t j = (qu - lo_u) >> dshift;
+    const int jj = j < (uint64_t)kDir ? (int)j : kDir - 1;
+    m = dir[jj];
+    hi = dir[jj + 1];
+  }
+  while (m < hi && st.kp[(m + 1) * KS] <= q) m++;
+  const int64_t *kr = st.kp + m * KS;
+  int c = 0;
+#pragma unroll
+  for (int step = LC / 2; step > 0; step >>= 1)
+    if (kr[c + step] <= q) c += step;
+  (void)nl;
+  return kr[c] == q ? st.vp[m * LC + c] : HM_NOT_FOUND;
+}
+
 template <int LC>
 __device__ __noinline__ int64_t lookup_scalar(const DevTree &t, int f, int64_t q) {
   constexpr int LI = LC >= 32 ? LC / 8 : 0;
@@ -185,11 +249,13 @@ __device__ __noinline__ int64_t lookup_scalar(const DevTree &t, int f, int64_t q
 // kRun queries per step.  Item descriptors are loaded kStages items ahead and
 // the queries of the next step (of this item or the next) one step ahead.
 // Results are written in the grouped order (out[i] for grouped query i).
-template <int LC>
+// DIR: each staged item first builds its directory (batches with many queries
+// per bucket); otherwise a query binary-searches the staged first keys.
+template <int LC, bool DIR>
 __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t, int f, const Item *__restrict__ items,
                                                         const int64_t *__restrict__ nitems,
                                                         const int64_t *__restrict__ qs, int64_t *__restrict__ out,
-                                                        int ml) {
+                                                        int ml, uint64_t key_lo_u, int shift) {
   static_assert(kStages >= 2, "a ring of at least two stages");
   extern __shared__ __align__(16) int64_t smem[];
   const int stage_words = ml * (2 * LC + 1);
@@ -198,6 +264,8 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
   int64_t it = blockIdx.x;
   if (it >= n_items) return;
   const Item none{0, 0, 0, 0};
+  __shared__ int32_t dir[DIR ? kDir + 1 : 1];
+  const int dshift = shift > kDirBits ? shift - kDirBits : 0;
   Item d[kStages];  // items it, it + g, ..., it + (kStages - 1) g
 #pragma unroll
   for (int x = 0; x < kStages; x++) d[x] = it + x * g < n_items ? items[it + x * g] : none;
@@ -210,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
 #pragma unroll
   for (int j = 0; j < kPerThread; j++) {
     const int r = j * kThreads + threadIdx.x;
-    q[j] = r < d[0].len ? __ldg(qs + d[0].qa + r) : 0;
+    q[j] = r < d[0].len() ? __ldg(qs + d[0].qa + r) : 0;
   }
   int cur_stage = 0;
   for (; it < n_items; it += g) {
@@ -222,14 +290,19 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
     __syncthreads();
     const Item cur = d[0];
     const Stage<LC> st(smem + cur_stage * stage_words, ml);
-    const bool staged = cur.nl >= 1 && cur.nl <= ml;
+    const bool staged = cur.nl() >= 1 && cur.nl() <= ml;
     int span = 1;
-    while (span < cur.nl) span <<= 1;
-    for (int r0 = 0; r0 < cur.len; r0 += kRun) {
+    while (span < cur.nl()) span <<= 1;
+    const uint64_t lo_u = key_lo_u + ((uint64_t)cur.b << shift);
+    if (DIR && staged) {  // uniform across the CTA
+      build_dir<LC>(st, cur.nl(), span, lo_u, dshift, dir);
+      __syncthreads();
+    }
+    for (int r0 = 0; r0 < cur.len(); r0 += kRun) {
       // the next step's queries: this item's next run, else the next item's first
-      const bool more = r0 + kRun < cur.len;
+      const bool more = r0 + kRun < cur.len();
       const int32_t na = more ? cur.qa + r0 + kRun : d[1].qa;
-      const int32_t nlen = more ? cur.len - r0 - kRun : d[1].len;
+      const int32_t nlen = more ? cur.len() - r0 - kRun : d[1].len();
       int64_t qn[kPerThread];
 #pragma unroll
       for (int j = 0; j < kPerThread; j++) {
@@ -239,9 +312,16 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
 #pragma unroll
       for (int j = 0; j < kPerThread; j++) {
         const int r = r0 + j * kThreads + threadIdx.x;
-        if (r >= cur.len) continue;
+        if (r >= cur.len()) continue;
         int64_t v = HM_NOT_FOUND;
-        if (q[j] != kMaxKey) v = staged ? lookup_staged<LC>(st, cur.nl, span, q[j]) : lookup_scalar<LC>(t, f, q[j]);
+        if (q[j] != kMaxKey) {
+          if (!staged)
+            v = lookup_scalar<LC>(t, f, q[j]);
+          else if (DIR)
+            v = lookup_dir<LC>(st, cur.nl(), dir, lo_u, dshift, q[j]);
+          else
+            v = lookup_staged<LC>(st, cur.nl(), span, q[j]);
+        }
         out[cur.qa + r] = v;  // grouped order: consecutive threads, consecutive slots
       }
 #pragma unroll
@@ -325,16 +405,16 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
   const size_t smem = (size_t)kStages * ml * leaf_bytes(lc);
   const int per_sm = std::max(1, std::min(8, (int)((227 * 1024) / (smem + 1024))));
   const unsigned grid = (unsigned)std::min<int64_t>(max_items(n, nb), (int64_t)t->num_sms * per_sm);
-  int rc = opt_in_smem(lc == 16 ? (const void *)join_kernel<16> : (const void *)join_kernel<64>,
-                       kStages * kStageMax);
+  // measured: the directory pays from about three queries per thread and item
+  const bool dir = HM_JOIN_DIR_BITS > 0 && n >= (int64_t)HM_JOIN_DIR_MIN * nb;
+  using Kernel = void (*)(DevTree, int, const Item *, const int64_t *, const int64_t *, int64_t *, int, uint64_t, int);
+  Kernel k = nullptr;
+  if (lc == 16) k = dir ? join_kernel<16, true> : join_kernel<16, false>;
+  else if (lc == 64) k = dir ? join_kernel<64, true> : join_kernel<64, false>;
+  else return HM_EINVAL;
+  int rc = opt_in_smem((const void *)k, kStages * kStageMax);
   if (rc) return rc;
-  if (lc == 16) {
-    join_kernel<16><<<grid, kThreads, smem, s>>>(t->view(), t->cfg.fanout, items, first + nb, qs, out, ml);
-  } else if (lc == 64) {
-    join_kernel<64><<<grid, kThreads, smem, s>>>(t->view(), t->cfg.fanout, items, first + nb, qs, out, ml);
-  } else {
-    return HM_EINVAL;
-  }
+  k<<<grid, kThreads, smem, s>>>(t->view(), t->cfg.fanout, items, first + nb, qs, out, ml, biased(t->key_min), shift);
   note_launch(3);
   return cuda_err(cudaGetLastError());
 }

@@ -36,7 +36,11 @@ namespace hm {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int64_t kChunk = 8192;  // queries per CTA chunk (offsets inside a chunk fit 16 bits)
+#ifndef HM_PSA_CHUNK
+#define HM_PSA_CHUNK 8192
+#endif
+constexpr int64_t kChunk = HM_PSA_CHUNK;  // queries per CTA chunk (offsets inside a chunk fit 16 bits)
+static_assert(kChunk <= 65536, "offsets inside a chunk are kept in 16 bits");
 #ifndef HM_PSA_TILE
 #define HM_PSA_TILE 8192  // queries a scatter CTA stages at a time (a divisor of kChunk)
 #endif
@@ -53,6 +57,15 @@ constexpr int kTile = HM_PSA_TILE;
 #define HM_PSA_REV_BATCH 2  // digit runs a warp of the inverse reads at once
 #endif
 constexpr int kRevThreads = HM_PSA_REV_THREADS;
+
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 
 // Bucket of a key: top `bits` bits of (k - lo) over the tree's key range.
 struct Bucket {
@@ -313,8 +326,9 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(
 // memory, then written to the chunk's input range in order.  The runs are cut
 // into units of 64 elements (a skewed batch can put most of a chunk in one
 // run); warps take units round-robin, a lane per element so every load is
-// one coalesced request, kRevBatch units at a time with all their loads
-// issued before the stores.
+// one coalesced request, kRevBatch units at a time: the offsets are loaded
+// first, then each result is copied from global memory straight to its slot
+// with cp.async.  The chunk is written out with 16-B stores when aligned.
 constexpr int kRevWarps = kRevThreads / 32;
 constexpr int kRevBatch = HM_PSA_REV_BATCH;
 #ifndef HM_PSA_REV_UNIT
@@ -370,36 +384,46 @@ __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_ke
   for (int d = tid; d < nd; d += kRevThreads)  // the run of every unit
     for (int u = up[d]; u < up[d + 1]; u++) unit_run[u] = (uint8_t)d;
   __syncthreads();
+  // Each result goes straight from global memory to its slot in shared memory
+  // (cp.async, 8 B) once its offset is known: only the offsets pass through
+  // registers, so a warp keeps the copies of many units in flight.
   for (int u0 = wid; u0 < units; u0 += kRevWarps * kRevBatch) {
-    int64_t r[kRevBatch][kUnitPer];
     uint16_t l[kRevBatch][kUnitPer];
+    int64_t a[kRevBatch];
     int cnt[kRevBatch];
 #pragma unroll
     for (int x = 0; x < kRevBatch; x++) {
       const int u = u0 + x * kRevWarps;
       cnt[x] = 0;
+      a[x] = 0;
       if (u < units) {
         const int d = unit_run[u];
         const int e0 = (u - up[d]) * kUnit;
-        const int64_t a = rs[d] + e0;
+        a[x] = rs[d] + e0;
         cnt[x] = min(kUnit, rl[d] - e0);
 #pragma unroll
-        for (int h = 0; h < kUnitPer; h++) {
-          if (lane + 32 * h < cnt[x]) {
-            r[x][h] = __ldg(res_in + a + lane + 32 * h);
-            l[x][h] = __ldg(loc + a + lane + 32 * h);
-          }
-        }
+        for (int h = 0; h < kUnitPer; h++)
+          if (lane + 32 * h < cnt[x]) l[x][h] = __ldg(loc + a[x] + lane + 32 * h);
       }
     }
 #pragma unroll
     for (int x = 0; x < kRevBatch; x++)
 #pragma unroll
       for (int h = 0; h < kUnitPer; h++)
-        if (lane + 32 * h < cnt[x]) staged[l[x][h]] = r[x][h];
+        if (lane + 32 * h < cnt[x]) cp_async8(staged + l[x][h], res_in + a[x] + lane + 32 * h);
   }
+  cp_async_wait_all();
   __syncthreads();
-  for (int x = tid; x < len; x += kRevThreads) dst[c.begin + x] = staged[x];
+  int64_t *o = dst + c.begin;
+  if ((reinterpret_cast<uintptr_t>(o) & 15) == 0) {  // 16-B stores, the odd tail element alone
+    const int pairs = len >> 1;
+    const longlong2 *sv = reinterpret_cast<const longlong2 *>(staged);
+    longlong2 *ov = reinterpret_cast<longlong2 *>(o);
+    for (int x = tid; x < pairs; x += kRevThreads) ov[x] = sv[x];
+    if ((len & 1) && tid == 0) o[len - 1] = staged[len - 1];
+  } else {
+    for (int x = tid; x < len; x += kRevThreads) o[x] = staged[x];
+  }
 }
 
 // One CTA: chunk descriptors for a pass.  bstart == nullptr: the whole input

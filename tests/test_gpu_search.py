@@ -233,15 +233,33 @@ def test_plan_replay_matches_and_follows_rebuild():
         plan.close()
 
 
+def bucket_edges(sk, n_leaf, count):
+    """Keys at and next to the first `count` bucket boundaries of the join
+    (top bits of key - key_min, as many bits as leave about 32 leaves per bucket)."""
+    bits = 1
+    while bits < 16 and (n_leaf >> bits) > 32:
+        bits += 1
+    lo, rng = int(sk[0]), (int(sk[-1]) - int(sk[0])) % (1 << 64)
+    shift = max(rng.bit_length() - bits, 0)
+    out = []
+    for b in range(count):
+        edge = lo + (b << shift)
+        out += [edge - 1, edge, edge + 1]
+    return np.array([min(max(x, -(2**63)), 2**63 - 1) for x in out], np.int64)
+
+
+@pytest.mark.parametrize("nq", [(1 << 19) + 77, (1 << 21) + 333])  # about 256 / 1024 queries per bucket
 @pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (128, 64)])
-def test_bucket_join_matches_oracle(fanout, leaf_cap):
+def test_bucket_join_matches_oracle(fanout, leaf_cap, nq):
     keys = dg.gen_keys(1 << 20, seed=81)
     sk = np.sort(keys)
     oracle = po.PortTree(sk, dg.values_for(sk))
     with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), fanout=fanout, leaf_cap=leaf_cap) as t:
         t.set_search_config(join=1)
-        q = dg.gen_point_queries(keys, (1 << 21) + 333, 0.7, seed=82)
+        q = dg.gen_point_queries(keys, nq, 0.7, seed=82)
         q[:6] = [sk[0], sk[-1], sk[0] - 1, sk[-1] + 1, -(2**63), 2**63 - 1]
+        edges = bucket_edges(sk, t.info().n_leaf, 300)
+        q[6:6 + len(edges)] = edges
         assert (t.search(cuda(q)).cpu().numpy() == oracle.search(q)).all()
         z = dg.gen_zipf_queries(sk, 1 << 21, 0.99, seed=83)  # hot buckets split into several runs
         assert (t.search(cuda(z)).cpu().numpy() == oracle.search(z)).all()
