@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
 #include <vector>
 
 #include "../../include/harmonia.h"
@@ -164,6 +165,41 @@ struct hm_tree {
 };
 
 namespace hm {
+
+// ---- programmatic dependent launch ----
+// Kernels of the search path are launched with programmatic stream
+// serialization: a kernel may be scheduled while its predecessor on the
+// stream drains, and waits for it (griddepcontrol.wait, a no-op for a normal
+// launch) before touching memory.  Each such kernel calls pdl_enter() first;
+// it also lets its own successor be scheduled (launch_dependents), which
+// happens once every CTA of this grid has started.
+#ifndef HM_PDL
+#define HM_PDL 1
+#endif
+__device__ __forceinline__ void pdl_enter() {
+#if HM_PDL
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
+// Launches kernel k on stream s with the programmatic-serialization
+// attribute (the kernel must call pdl_enter() before any memory access).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = HM_PDL;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
 
 // ---- radix sort (sort.cu) ----
 // Stable LSD sort of (ukeys, vals) by bits [begin_bit, end_bit) of the

@@ -64,6 +64,7 @@ struct __align__(16) Item {
 __global__ void bucket_prep_kernel(DevTree t, int f, int64_t lo, int shift, int nb,
                                    const int64_t *__restrict__ bstart, int32_t *__restrict__ leafb,
                                    int32_t *__restrict__ cnt) {
+  pdl_enter();
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x) {
     cnt[b] = b < nb ? (int32_t)((bstart[b + 1] - bstart[b] + kItemMax - 1) / kItemMax) : 0;
     if (b == 0) {
@@ -87,6 +88,7 @@ __global__ void bucket_prep_kernel(DevTree t, int f, int64_t lo, int shift, int 
 __global__ void expand_items_kernel(int nb, const int64_t *__restrict__ bstart, const int32_t *__restrict__ leafb,
                                     const int32_t *__restrict__ cnt, const int64_t *__restrict__ first,
                                     Item *__restrict__ items) {
+  pdl_enter();
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
     const int c = cnt[b];
     if (c == 0) continue;
@@ -256,6 +258,7 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
                                                         const int64_t *__restrict__ nitems,
                                                         const int64_t *__restrict__ qs, int64_t *__restrict__ out,
                                                         int ml, uint64_t key_lo_u, int shift) {
+  pdl_enter();
   static_assert(kStages >= 2, "a ring of at least two stages");
   extern __shared__ __align__(16) int64_t smem[];
   const int stage_words = ml * (2 * LC + 1);
@@ -397,9 +400,9 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
   while (len < 64 && (range >> len) != 0) len++;
   const int shift = len > bits ? len - bits : 0;
   const unsigned gb = (unsigned)((nb + 1 + 255) / 256);
-  bucket_prep_kernel<<<gb, 256, 0, s>>>(t->view(), t->cfg.fanout, t->key_min, shift, nb, bstart, leafb, cnt);
+  launch_pdl(bucket_prep_kernel, gb, 256, 0, s, t->view(), t->cfg.fanout, t->key_min, shift, nb, bstart, leafb, cnt);
   exclusive_scan_i32(cnt, first, nb + 1, scan, s);
-  expand_items_kernel<<<gb, 256, 0, s>>>(nb, bstart, leafb, cnt, first, items);
+  launch_pdl(expand_items_kernel, gb, 256, 0, s, nb, bstart, leafb, cnt, first, items);
   const int lc = t->cfg.leaf_cap;
   const int ml = stage_leaves_for(t, bits);
   const size_t smem = (size_t)kStages * ml * leaf_bytes(lc);
@@ -414,7 +417,8 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
   else return HM_EINVAL;
   int rc = opt_in_smem((const void *)k, kStages * kStageMax);
   if (rc) return rc;
-  k<<<grid, kThreads, smem, s>>>(t->view(), t->cfg.fanout, items, first + nb, qs, out, ml, biased(t->key_min), shift);
+  launch_pdl(k, grid, kThreads, smem, s, t->view(), t->cfg.fanout, items, first + nb, qs, out, ml, biased(t->key_min),
+             shift);
   note_launch(3);
   return cuda_err(cudaGetLastError());
 }

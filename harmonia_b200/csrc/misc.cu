@@ -31,6 +31,7 @@ constexpr int kScanStep = kThreads * kScanPer;  // elements per CTA per scan ste
 template <typename T>
 __global__ void __launch_bounds__(kThreads) seg_sum_kernel(const T *__restrict__ in, int64_t n,
                                                            int64_t seg, int64_t *__restrict__ part) {
+  pdl_enter();
   __shared__ int64_t red[kThreads / 32];
   int64_t b0 = (int64_t)blockIdx.x * seg, b1 = min(n, b0 + seg);
   int64_t s = 0;
@@ -62,6 +63,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) seg_scan_kernel(const T *__restrict__ in, int64_t n,
                                                             int64_t seg, const int64_t *__restrict__ part,
                                                             int64_t *__restrict__ out, int nctas) {
+  pdl_enter();
   __shared__ int64_t buf[kScanStep + kScanStep / 8];
   __shared__ int64_t wsum[kThreads / 32];
   __shared__ int64_t carry;
@@ -201,9 +203,9 @@ void exclusive_scan(const T *in, int64_t *out, int64_t n, void *scratch, cudaStr
     cudaMemsetAsync(out, 0, sizeof(int64_t), s);
     return;
   }
-  seg_sum_kernel<T><<<nctas, kThreads, 0, s>>>(in, n, seg, part);
+  launch_pdl(seg_sum_kernel<T>, nctas, kThreads, 0, s, in, n, seg, part);
   scan_counts(part, nctas, s);
-  seg_scan_kernel<T><<<nctas, kThreads, 0, s>>>(in, n, seg, part, out, nctas);
+  launch_pdl(seg_scan_kernel<T>, nctas, kThreads, 0, s, in, n, seg, part, out, nctas);
   note_launch(2);
 }
 

@@ -110,6 +110,7 @@ struct ChunkIO {
 __global__ void __launch_bounds__(1024) batch_chunk_kernel(BatchView bv, Chunk *__restrict__ chunks,
                                                             int32_t *__restrict__ nchunks_total,
                                                             ChunkIO *__restrict__ cio) {
+  pdl_enter();
   __shared__ int32_t pre[1024];
   const int tid = threadIdx.x, nb = bv.nb;
   const int per = (nb + 1023) / 1024;
@@ -159,8 +160,13 @@ __global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__res
                                                         const Chunk *__restrict__ chunks,
                                                         const int32_t *__restrict__ nchunks_total, Bucket bk,
                                                         int shift2, int mask2, int64_t *__restrict__ counts) {
+  pdl_enter();
   __shared__ unsigned hist[256];
-  if ((int)blockIdx.x >= *nchunks_total) return;
+  if ((int)blockIdx.x >= *nchunks_total) {
+    // the counts of the chunks this launch does not have stay zero for the scan
+    for (int d = threadIdx.x; d < 256; d += kThreads) counts[(int64_t)blockIdx.x * 256 + d] = 0;
+    return;
+  }
   const Chunk c = chunks[blockIdx.x];
   const int64_t *src = BATCHED ? cio[blockIdx.x].qbase : q;  // a chunk lies inside one batch
   for (int i = threadIdx.x; i < 256; i += kThreads) hist[i] = 0;
@@ -177,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__res
       if (base + j * kThreads + threadIdx.x < c.end) atomicAdd(&hist[(bk(k[j]) >> shift2) & mask2], 1u);
   }
   __syncthreads();
-  for (int d = threadIdx.x; d <= mask2; d += kThreads) counts[count_index(c, d)] = hist[d];
+  for (int d = threadIdx.x; d < 256; d += kThreads) counts[count_index(c, d)] = hist[d];  // 0 past mask2
 }
 
 // Scatter of one pass.  A grid of resident CTAs takes chunks from a counter
@@ -205,6 +211,7 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(
     const int64_t *__restrict__ q, const ChunkIO *__restrict__ cio, const T *__restrict__ pay_in,
     const Chunk *__restrict__ chunks, int32_t *__restrict__ nchunks_total, Bucket bk, int shift2, int mask2,
     const int64_t *__restrict__ offs, int64_t *__restrict__ q_out, T *__restrict__ pay_out) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char dyn[];
   int64_t *skey = reinterpret_cast<int64_t *>(dyn);                 // grouped keys
   uint32_t *saux = reinterpret_cast<uint32_t *>(dyn + 8 * kTile);  // digit << 16 | tile position
@@ -342,6 +349,7 @@ __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_ke
     const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total, const int64_t *__restrict__ offs,
     int nd, const int64_t *__restrict__ res_in, const uint16_t *__restrict__ loc, int64_t *__restrict__ res_out,
     BatchView bv, const ChunkIO *__restrict__ cio) {
+  pdl_enter();
   extern __shared__ __align__(16) int64_t staged[];  // kChunk results
   __shared__ int64_t rs[256];
   __shared__ int32_t rl[256];
@@ -431,6 +439,7 @@ __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_ke
 // split into chunks of at most kChunk queries; chunks are ordered by bucket.
 __global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__ bstart, int nb, int64_t n,
                                                      Chunk *__restrict__ chunks, int32_t *__restrict__ nchunks_total) {
+  pdl_enter();
   __shared__ int32_t pre[1024];
   const int tid = threadIdx.x;
   if (!bstart) {  // one bucket: the whole input
@@ -494,6 +503,7 @@ __global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__
 __global__ void bucket_starts_kernel(const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total,
                                      const int64_t *__restrict__ offs, int nb, int nd, int64_t n,
                                      const int64_t *__restrict__ bstart_in, int64_t *__restrict__ bstart) {
+  pdl_enter();
   const int total = nb * nd;
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x <= total; x += gridDim.x * blockDim.x) {
     if (x == total) {
@@ -586,19 +596,18 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
               int shift2, int mask2, int64_t *q_out, T *pay_out, int64_t *bstart_out, const Pass &ps, void *scan,
               int sms, cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
   if (BATCHED)
-    batch_chunk_kernel<<<1, 1024, 0, s>>>(bv, ps.chunks, ps.nchunks, const_cast<ChunkIO *>(cio));
+    launch_pdl(batch_chunk_kernel, 1, 1024, 0, s, bv, ps.chunks, ps.nchunks, const_cast<ChunkIO *>(cio));
   else
-    chunk_kernel<<<1, 1024, 0, s>>>(bstart_in, nb, n, ps.chunks, ps.nchunks);
-  cudaMemsetAsync(ps.offs, 0, sizeof(int64_t) * (256 * ps.mc + 1), s);
-  psa_hist_kernel<BATCHED><<<(unsigned)ps.mc, kThreads, 0, s>>>(q, bv, cio, ps.chunks, ps.nchunks, bk, shift2,
+    launch_pdl(chunk_kernel, 1, 1024, 0, s, bstart_in, nb, n, ps.chunks, ps.nchunks);
+  launch_pdl(psa_hist_kernel<BATCHED>, (unsigned)ps.mc, kThreads, 0, s, q, bv, cio, ps.chunks, ps.nchunks, bk, shift2,
                                                                  mask2, ps.offs);
   exclusive_scan_i64(ps.offs, ps.offs, 256 * ps.mc, scan, s);
   opt_in_smem((const void *)psa_scatter_kernel<T, LOAD, BATCHED>, stage_bytes());
   const unsigned grid = (unsigned)std::min<int64_t>(ps.mc, (int64_t)sms * HM_PSA_SCATTER_MINB);
-  psa_scatter_kernel<T, LOAD, BATCHED><<<grid, kSc, stage_bytes(), s>>>(q, cio, pay_in, ps.chunks, ps.nchunks, bk,
+  launch_pdl(psa_scatter_kernel<T, LOAD, BATCHED>, grid, kSc, stage_bytes(), s, q, cio, pay_in, ps.chunks, ps.nchunks, bk,
                                                                          shift2, mask2, ps.offs, q_out, pay_out);
   const int nd = mask2 + 1;
-  bucket_starts_kernel<<<(unsigned)((nb * nd + 256) / 256), 256, 0, s>>>(ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
+  launch_pdl(bucket_starts_kernel, (unsigned)((nb * nd + 256) / 256), 256, 0, s, ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
                                                                          bstart_in, bstart_out);
   note_launch(4);  // chunk, histogram, scatter, bucket starts (the scan counts its own)
 }
@@ -607,7 +616,7 @@ template <bool BATCHED = false>
 void unpermute_pass(const Pass &ps, int nd, const int64_t *res_in, const uint16_t *loc, int64_t *res_out,
                     cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
   opt_in_smem((const void *)psa_unpermute_kernel<BATCHED>, (int)(8 * kChunk));
-  psa_unpermute_kernel<BATCHED><<<(unsigned)ps.mc, kRevThreads, 8 * kChunk, s>>>(ps.chunks, ps.nchunks, ps.offs, nd,
+  launch_pdl(psa_unpermute_kernel<BATCHED>, (unsigned)ps.mc, kRevThreads, 8 * kChunk, s, ps.chunks, ps.nchunks, ps.offs, nd,
                                                                                  res_in, loc, res_out, bv, cio);
   note_launch();
 }

@@ -14,6 +14,7 @@ namespace {
 
 // One-CTA in-place exclusive scan (small arrays).
 __global__ void __launch_bounds__(1024) scan_counts_kernel(int64_t *counts, int64_t m) {
+  pdl_enter();
   __shared__ int64_t part[1024];
   int64_t per = (m + 1023) / 1024;
   int64_t b0 = (int64_t)threadIdx.x * per, b1 = min(m, b0 + per);
@@ -47,7 +48,7 @@ struct RadixDigit {
 // m + 1 entries plus scan_scratch_bytes(m) bytes after them.
 void scan_counts(int64_t *counts, int64_t m, cudaStream_t s) {
   if (m <= 4096) {
-    scan_counts_kernel<<<1, 1024, 0, s>>>(counts, m);
+    launch_pdl(scan_counts_kernel, 1, 1024, 0, s, counts, m);
     note_launch();
     return;
   }
