@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(kThreads) seg_sum_kernel(const T *__restrict__
   }
 }
 
-// Exclusive scan of each segment, offset by the scanned segment sums.  A step
+// Exclusive scan of each segment, offset by the sum of the segments before it
+// (each CTA adds up those of the at most 592 segment sums itself).  A step
 // stages kScanStep elements in shared memory (coalesced), each thread scans
 // kScanPer consecutive ones (index i at i + i / 8: one pad word per 8 keeps
 // the threads' runs in different banks), one block scan of the thread sums.
@@ -69,7 +70,19 @@ __global__ void __launch_bounds__(kThreads) seg_scan_kernel(const T *__restrict_
   __shared__ int64_t carry;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int64_t b0 = (int64_t)blockIdx.x * seg, b1 = min(n, b0 + seg);
-  if (tid == 0) carry = part[blockIdx.x];
+  {
+    int64_t before = 0;
+    for (int i = tid; i < (int)blockIdx.x; i += kThreads) before += part[i];
+    for (int o = 16; o; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
+    if (lane == 0) wsum[warp] = before;
+    __syncthreads();
+    if (tid == 0) {
+      int64_t c = 0;
+      for (int w = 0; w < kThreads / 32; w++) c += wsum[w];
+      carry = c;
+    }
+    __syncthreads();
+  }
   for (int64_t base = b0; base < b1; base += kScanStep) {
 #pragma unroll
     for (int j = 0; j < kScanPer; j++) {
@@ -204,12 +217,10 @@ void exclusive_scan(const T *in, int64_t *out, int64_t n, void *scratch, cudaStr
     return;
   }
   launch_pdl(seg_sum_kernel<T>, nctas, kThreads, 0, s, in, n, seg, part);
-  scan_counts(part, nctas, s);
   launch_pdl(seg_scan_kernel<T>, nctas, kThreads, 0, s, in, n, seg, part, out, nctas);
   note_launch(2);
 }
 
-void scan_counts(int64_t *counts, int64_t m, cudaStream_t s);
 
 void exclusive_scan_i64(const int64_t *in, int64_t *out, int64_t n, void *scratch, cudaStream_t s) {
   exclusive_scan<int64_t>(in, out, n, scratch, s);

@@ -109,7 +109,7 @@ struct ChunkIO {
 // One CTA: the batch set's first-pass chunks and their ChunkIO.
 __global__ void __launch_bounds__(1024) batch_chunk_kernel(BatchView bv, Chunk *__restrict__ chunks,
                                                             int32_t *__restrict__ nchunks_total,
-                                                            ChunkIO *__restrict__ cio) {
+                                                            int32_t *__restrict__ bfirst, ChunkIO *__restrict__ cio) {
   pdl_enter();
   __shared__ int32_t pre[1024];
   const int tid = threadIdx.x, nb = bv.nb;
@@ -152,6 +152,7 @@ __global__ void __launch_bounds__(1024) batch_chunk_kernel(BatchView bv, Chunk *
   if (tid == 1023) {
     nchunks_total[0] = total;
     nchunks_total[1] = 0;  // work counter of the persistent scatter
+    bfirst[0] = total > 0 ? 0 : -1;
   }
 }
 
@@ -438,7 +439,8 @@ __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_ke
 // as one bucket (nb = 1).  Otherwise every bucket [bstart[b], bstart[b+1]) of nb is
 // split into chunks of at most kChunk queries; chunks are ordered by bucket.
 __global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__ bstart, int nb, int64_t n,
-                                                     Chunk *__restrict__ chunks, int32_t *__restrict__ nchunks_total) {
+                                                     Chunk *__restrict__ chunks, int32_t *__restrict__ nchunks_total,
+                                                     int32_t *__restrict__ bfirst) {
   pdl_enter();
   __shared__ int32_t pre[1024];
   const int tid = threadIdx.x;
@@ -457,6 +459,7 @@ __global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__
     if (tid == 0) {
       nchunks_total[0] = nc;
       nchunks_total[1] = 0;  // work counter of the persistent scatter
+      bfirst[0] = nc > 0 ? 0 : -1;
     }
     return;
   }
@@ -480,6 +483,7 @@ __global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__
     if (b >= nb) break;
     const int64_t s = bstart[b], e = bstart[b + 1];
     const int32_t nc = (int32_t)((e - s + kChunk - 1) / kChunk);
+    bfirst[b] = nc > 0 ? base : -1;
     for (int32_t i = 0; i < nc; i++) {
       Chunk c;
       c.begin = s + (int64_t)i * kChunk;
@@ -499,8 +503,9 @@ __global__ void __launch_bounds__(1024) chunk_kernel(const int64_t *__restrict__
 }
 
 // Starts of the pass's output buckets: bucket (b, d) starts at the offset of
-// digit d in b's first chunk; an empty input bucket b starts where it did.
-__global__ void bucket_starts_kernel(const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total,
+// digit d in b's first chunk (bfirst, from the chunk kernel); an empty input
+// bucket b starts where it did.
+__global__ void bucket_starts_kernel(const Chunk *__restrict__ chunks, const int32_t *__restrict__ bfirst,
                                      const int64_t *__restrict__ offs, int nb, int nd, int64_t n,
                                      const int64_t *__restrict__ bstart_in, int64_t *__restrict__ bstart) {
   pdl_enter();
@@ -511,17 +516,7 @@ __global__ void bucket_starts_kernel(const Chunk *__restrict__ chunks, const int
       continue;
     }
     const int b = x / nd, d = x % nd;
-    int lo = 0, hi = *nchunks_total - 1, first = -1;
-    while (lo <= hi) {  // first chunk of bucket b
-      const int mid = (lo + hi) >> 1;
-      const int mb = chunks[mid].bucket;
-      if (mb < b) {
-        lo = mid + 1;
-      } else {
-        if (mb == b) first = mid;
-        hi = mid - 1;
-      }
-    }
+    const int first = bfirst[b];
     bstart[x] = first >= 0 ? offs[count_index(chunks[first], d)] : (bstart_in ? bstart_in[b] : 0);
   }
 }
@@ -544,7 +539,8 @@ int64_t max_chunks(int64_t n, int nb) { return (n + kChunk - 1) / kChunk + nb + 
 struct Pass {
   Chunk *chunks;
   int32_t *nchunks;
-  int64_t *offs;  // 256 * mc + 1
+  int32_t *bfirst;  // first chunk of each input bucket, -1 for an empty one (at most 256)
+  int64_t *offs;    // 256 * mc + 1
   int64_t mc;
 };
 
@@ -573,11 +569,13 @@ size_t work_layout(int64_t n, int bits, bool offsets, Work *w, char *base, int b
   x.p1.mc = mc1;
   x.p1.chunks = reinterpret_cast<Chunk *>(take(sizeof(Chunk) * mc1));
   x.p1.nchunks = reinterpret_cast<int32_t *>(take(16));
+  x.p1.bfirst = reinterpret_cast<int32_t *>(take(4 * 256));
   x.p1.offs = reinterpret_cast<int64_t *>(take(8 * (256 * mc1 + 1)));
   if (two) {
     x.p2.mc = mc2;
     x.p2.chunks = reinterpret_cast<Chunk *>(take(sizeof(Chunk) * mc2));
     x.p2.nchunks = reinterpret_cast<int32_t *>(take(16));
+    x.p2.bfirst = reinterpret_cast<int32_t *>(take(4 * 256));
     x.p2.offs = reinterpret_cast<int64_t *>(take(8 * (256 * mc2 + 1)));
   }
   x.scan = take(scan_scratch_bytes(256 * std::max(mc1, mc2)));
@@ -596,9 +594,9 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
               int shift2, int mask2, int64_t *q_out, T *pay_out, int64_t *bstart_out, const Pass &ps, void *scan,
               int sms, cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
   if (BATCHED)
-    launch_pdl(batch_chunk_kernel, 1, 1024, 0, s, bv, ps.chunks, ps.nchunks, const_cast<ChunkIO *>(cio));
+    launch_pdl(batch_chunk_kernel, 1, 1024, 0, s, bv, ps.chunks, ps.nchunks, ps.bfirst, const_cast<ChunkIO *>(cio));
   else
-    launch_pdl(chunk_kernel, 1, 1024, 0, s, bstart_in, nb, n, ps.chunks, ps.nchunks);
+    launch_pdl(chunk_kernel, 1, 1024, 0, s, bstart_in, nb, n, ps.chunks, ps.nchunks, ps.bfirst);
   launch_pdl(psa_hist_kernel<BATCHED>, (unsigned)ps.mc, kThreads, 0, s, q, bv, cio, ps.chunks, ps.nchunks, bk, shift2,
                                                                  mask2, ps.offs);
   exclusive_scan_i64(ps.offs, ps.offs, 256 * ps.mc, scan, s);
@@ -607,7 +605,7 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
   launch_pdl(psa_scatter_kernel<T, LOAD, BATCHED>, grid, kSc, stage_bytes(), s, q, cio, pay_in, ps.chunks, ps.nchunks, bk,
                                                                          shift2, mask2, ps.offs, q_out, pay_out);
   const int nd = mask2 + 1;
-  launch_pdl(bucket_starts_kernel, (unsigned)((nb * nd + 256) / 256), 256, 0, s, ps.chunks, ps.nchunks, ps.offs, nb, nd, n,
+  launch_pdl(bucket_starts_kernel, (unsigned)((nb * nd + 256) / 256), 256, 0, s, ps.chunks, ps.bfirst, ps.offs, nb, nd, n,
                                                                          bstart_in, bstart_out);
   note_launch(4);  // chunk, histogram, scatter, bucket starts (the scan counts its own)
 }
