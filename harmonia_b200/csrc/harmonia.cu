@@ -194,6 +194,8 @@ int free_tree(hm_tree *t) {
   cudaDeviceSynchronize();
   if (t->arena) cudaFree(t->arena);
   if (t->child_ids) cudaFree(t->child_ids);
+  if (t->join_leafb) cudaFree(t->join_leafb);
+  if (t->join_leafb_ready) cudaEventDestroy(t->join_leafb_ready);
   if (t->scratch) cudaFree(t->scratch);
   if (t->d_err) cudaFree(t->d_err);
   if (t->pinned) cudaFreeHost(t->pinned);

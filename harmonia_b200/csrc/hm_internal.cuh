@@ -117,6 +117,17 @@ struct hm_tree {
   int num_sms = 148;
   int64_t key_min = 0, key_max = 0;  // for the pre-sort digit
   uint64_t generation = 0;           // bumped when the arena is rebuilt
+  uint64_t shape_version = 0;        // bumped when inner nodes change in place (subtree rebalance)
+  // bucket join: the leaf of every bucket boundary, kept for the current
+  // shape, key range and bucket bits (join.cu); written on the stream of the
+  // search that filled it, join_leafb_ready recorded after it
+  mutable int32_t *join_leafb = nullptr;
+  mutable int64_t join_leafb_cap = 0;
+  mutable bool join_leafb_valid = false;
+  mutable uint64_t join_leafb_gen = 0, join_leafb_shape = 0;
+  mutable int64_t join_leafb_lo = 0, join_leafb_hi = 0, join_leafb_nleaf = 0;
+  mutable int join_leafb_bits = 0;
+  mutable cudaEvent_t join_leafb_ready = nullptr;
   int64_t join_tuned_min = INT64_MAX;  // smallest batch the autotuner saw the join win
   // comparison baseline (hm_search_baseline): children ids per inner node
   int32_t *child_ids = nullptr;

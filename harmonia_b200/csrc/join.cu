@@ -58,15 +58,18 @@ struct __align__(16) Item {
   __host__ __device__ int nl() const { return (int)(len_nl & 0xffffu); }
 };
 
-// Per bucket b in [0, nb]: leafb[b] = leaf holding the smallest key of bucket
-// b (bucket b's keys lie in leaves [leafb[b], leafb[b+1]]) and cnt[b] = its
-// work items (0 for b = nb).
+// Per bucket b in [0, nb]: cnt[b] = its work items (0 for b = nb) and, with
+// want_leafb, leafb[b] = leaf holding the smallest key of bucket b (bucket
+// b's keys lie in leaves [leafb[b], leafb[b+1]]).  leafb depends only on the
+// inner nodes, the key range and the bucket bits, so the launcher keeps it
+// per tree shape and skips the descents while that holds.
 __global__ void bucket_prep_kernel(DevTree t, int f, int64_t lo, int shift, int nb,
                                    const int64_t *__restrict__ bstart, int32_t *__restrict__ leafb,
-                                   int32_t *__restrict__ cnt) {
+                                   int32_t *__restrict__ cnt, bool want_leafb) {
   pdl_enter();
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x) {
     cnt[b] = b < nb ? (int32_t)((bstart[b + 1] - bstart[b] + kItemMax - 1) / kItemMax) : 0;
+    if (!want_leafb) continue;
     if (b == 0) {
       leafb[0] = 0;
       continue;
@@ -400,7 +403,54 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
   while (len < 64 && (range >> len) != 0) len++;
   const int shift = len > bits ? len - bits : 0;
   const unsigned gb = (unsigned)((nb + 1 + 255) / 256);
-  launch_pdl(bucket_prep_kernel, gb, 256, 0, s, t->view(), t->cfg.fanout, t->key_min, shift, nb, bstart, leafb, cnt);
+  // the boundaries' leaves: kept per tree shape (not inside a graph capture,
+  // whose replays must follow later changes of the tree)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = cudaStreamCaptureStatusActive;
+  }
+  bool want_leafb = true;
+  bool fill_cache = false;
+  if (cap == cudaStreamCaptureStatusNone) {
+    const bool same = t->join_leafb_valid && t->join_leafb_gen == t->generation &&
+                      t->join_leafb_shape == t->shape_version && t->join_leafb_lo == t->key_min &&
+                      t->join_leafb_hi == t->key_max && t->join_leafb_nleaf == t->n_leaf && t->join_leafb_bits == bits;
+    if (same) {
+      leafb = t->join_leafb;
+      want_leafb = false;
+      cudaStreamWaitEvent(s, t->join_leafb_ready, 0);
+    } else {
+      t->join_leafb_valid = false;
+      bool ok = true;
+      if (t->join_leafb_cap < nb + 1) {
+        if (t->join_leafb) cudaFree(t->join_leafb);
+        t->join_leafb = nullptr;
+        t->join_leafb_cap = 0;
+        ok = cudaMalloc(&t->join_leafb, 4 * (size_t)(nb + 1)) == cudaSuccess;
+        if (ok) t->join_leafb_cap = nb + 1;
+      }
+      if (ok && !t->join_leafb_ready)
+        ok = cudaEventCreateWithFlags(&t->join_leafb_ready, cudaEventDisableTiming) == cudaSuccess;
+      if (ok) {
+        leafb = t->join_leafb;
+        fill_cache = true;
+      } else {
+        cudaGetLastError();  // no cache: the boundaries are computed into scratch as in a capture
+      }
+    }
+  }
+  launch_pdl(bucket_prep_kernel, gb, 256, 0, s, t->view(), t->cfg.fanout, t->key_min, shift, nb, bstart, leafb, cnt,
+             want_leafb);
+  if (fill_cache && cudaEventRecord(t->join_leafb_ready, s) == cudaSuccess) {
+    t->join_leafb_valid = true;
+    t->join_leafb_gen = t->generation;
+    t->join_leafb_shape = t->shape_version;
+    t->join_leafb_lo = t->key_min;
+    t->join_leafb_hi = t->key_max;
+    t->join_leafb_nleaf = t->n_leaf;
+    t->join_leafb_bits = bits;
+  }
   exclusive_scan_i32(cnt, first, nb + 1, scan, s);
   launch_pdl(expand_items_kernel, gb, 256, 0, s, nb, bstart, leafb, cnt, first, items);
   const int lc = t->cfg.leaf_cap;

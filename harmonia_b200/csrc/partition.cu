@@ -156,19 +156,42 @@ __global__ void __launch_bounds__(1024) batch_chunk_kernel(BatchView bv, Chunk *
   }
 }
 
+// Digit counts of one chunk per CTA.  whole_n >= 0: the input is one bucket
+// of whole_n queries cut into kChunk pieces, and this kernel writes that
+// chunk table itself (no chunk kernel before it).
 template <bool BATCHED>
 __global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__restrict__ q, BatchView bv, const ChunkIO *__restrict__ cio,
-                                                        const Chunk *__restrict__ chunks,
-                                                        const int32_t *__restrict__ nchunks_total, Bucket bk,
+                                                        Chunk *__restrict__ chunks,
+                                                        int32_t *__restrict__ nchunks_total,
+                                                        int32_t *__restrict__ bfirst, int64_t whole_n, Bucket bk,
                                                         int shift2, int mask2, int64_t *__restrict__ counts) {
   pdl_enter();
   __shared__ unsigned hist[256];
-  if ((int)blockIdx.x >= *nchunks_total) {
+  const int nct = whole_n >= 0 ? (int)((whole_n + kChunk - 1) / kChunk) : *nchunks_total;
+  if ((int)blockIdx.x >= nct) {
     // the counts of the chunks this launch does not have stay zero for the scan
     for (int d = threadIdx.x; d < 256; d += kThreads) counts[(int64_t)blockIdx.x * 256 + d] = 0;
     return;
   }
-  const Chunk c = chunks[blockIdx.x];
+  Chunk c;
+  if (whole_n >= 0) {
+    c.begin = (int64_t)blockIdx.x * kChunk;
+    c.end = min(whole_n, c.begin + kChunk);
+    c.bucket = 0;
+    c.idx = (int32_t)blockIdx.x;
+    c.nchunks = nct;
+    c.base = 0;
+    if (threadIdx.x == 0) {
+      chunks[blockIdx.x] = c;
+      if (blockIdx.x == 0) {
+        nchunks_total[0] = nct;
+        nchunks_total[1] = 0;  // work counter of the persistent scatter
+        bfirst[0] = 0;
+      }
+    }
+  } else {
+    c = chunks[blockIdx.x];
+  }
   const int64_t *src = BATCHED ? cio[blockIdx.x].qbase : q;  // a chunk lies inside one batch
   for (int i = threadIdx.x; i < 256; i += kThreads) hist[i] = 0;
   __syncthreads();
@@ -593,11 +616,14 @@ template <typename T, bool LOAD, bool BATCHED = false>
 void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, const int64_t *bstart_in, int nb,
               int shift2, int mask2, int64_t *q_out, T *pay_out, int64_t *bstart_out, const Pass &ps, void *scan,
               int sms, cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
+  // a single unbatched input: the histogram kernel writes the chunk table
+  const bool whole = !BATCHED && bstart_in == nullptr;
   if (BATCHED)
     launch_pdl(batch_chunk_kernel, 1, 1024, 0, s, bv, ps.chunks, ps.nchunks, ps.bfirst, const_cast<ChunkIO *>(cio));
-  else
+  else if (!whole)
     launch_pdl(chunk_kernel, 1, 1024, 0, s, bstart_in, nb, n, ps.chunks, ps.nchunks, ps.bfirst);
-  launch_pdl(psa_hist_kernel<BATCHED>, (unsigned)ps.mc, kThreads, 0, s, q, bv, cio, ps.chunks, ps.nchunks, bk, shift2,
+  launch_pdl(psa_hist_kernel<BATCHED>, (unsigned)ps.mc, kThreads, 0, s, q, bv, cio, ps.chunks, ps.nchunks, ps.bfirst,
+             whole ? n : (int64_t)-1, bk, shift2,
                                                                  mask2, ps.offs);
   exclusive_scan_i64(ps.offs, ps.offs, 256 * ps.mc, scan, s);
   opt_in_smem((const void *)psa_scatter_kernel<T, LOAD, BATCHED>, stage_bytes());
@@ -607,7 +633,7 @@ void one_pass(const Bucket &bk, const int64_t *q, const T *pay_in, int64_t n, co
   const int nd = mask2 + 1;
   launch_pdl(bucket_starts_kernel, (unsigned)((nb * nd + 256) / 256), 256, 0, s, ps.chunks, ps.bfirst, ps.offs, nb, nd, n,
                                                                          bstart_in, bstart_out);
-  note_launch(4);  // chunk, histogram, scatter, bucket starts (the scan counts its own)
+  note_launch(whole ? 3 : 4);  // [chunk,] histogram, scatter, bucket starts (the scan counts its own)
 }
 
 template <bool BATCHED = false>

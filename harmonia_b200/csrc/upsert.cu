@@ -670,6 +670,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
           t->inner, t->prefix, t->leaf_rows, t->leaf_cnt, t->leaf_base, t->cfg.fanout, lc, li, g, mark, mk, mv, ml,
           nm);
       note_launch();
+      t->shape_version++;  // separators of the last inner level changed
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_err(e);
     }

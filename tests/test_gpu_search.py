@@ -285,7 +285,11 @@ def test_bucket_join_skewed_keys_fall_back(ends):
 def test_bucket_join_after_upserts(c1):
     keys, sk, _ = c1
     with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), leaf_fill=12) as t:
+        t.set_search_config(join=1)
+        q0 = dg.gen_point_queries(keys, 1 << 18, 0.8, seed=90)
+        assert (t.search(cuda(q0)).cpu().numpy() == po.PortTree(sk, dg.values_for(sk)).search(q0)).all()
         bk, bv = dg.gen_upserts(keys, 5000, 0.5, seed=91)
+        bk[:2] = [int(sk[0]) - 12345, min(int(sk[-1]) + 12345, 2**63 - 2)]  # new smallest and largest keys
         t.upsert(bk, bv)
         ek, ev = po.upsert_set(sk, dg.values_for(sk), bk, bv)
         q = np.concatenate([bk, dg.gen_point_queries(ek, 1 << 20, 0.8, seed=92)])

@@ -131,6 +131,9 @@ def test_overflowing_leaf_rebalances_its_subtree(fanout, leaf_cap, fill):
         info0 = t.info()
         q = dg.gen_point_queries(sk, 1 << 15, 0.8, seed=62)
         dq, dout = cuda(q), torch.empty(len(q), dtype=torch.int64, device="cuda")
+        t.set_search_config(join=1)  # the join keeps its bucket boundaries per tree shape
+        assert (t.search(dq).cpu().numpy() == po.PortTree(sk, sv).search(q)).all()
+        t.set_search_config(join=-1)
         with t.plan([(dq, dout)]) as plan:
             ek, ev = sk, sv
             for epoch, at in enumerate((5000, 5000, 70000)):
@@ -152,6 +155,9 @@ def test_overflowing_leaf_rebalances_its_subtree(fanout, leaf_cap, fill):
                 oracle = po.PortTree(ek, ev)
                 q2 = np.concatenate([bk, q])
                 assert (t.search(cuda(q2)).cpu().numpy() == oracle.search(q2)).all()
+                t.set_search_config(join=1)  # after the in-place rebalance
+                assert (t.search(cuda(q2)).cpu().numpy() == oracle.search(q2)).all()
+                t.set_search_config(join=-1)
                 st, ln = dg.gen_ranges(2000, 1, 200, seed=63 + epoch)
                 st[:50] = bk[:50] if len(bk) >= 50 else st[:50]
                 got = t.range_search(st, ln)
