@@ -30,7 +30,7 @@ namespace {
 
 constexpr int kThreads = 256;
 #ifndef HM_JOIN_PER_THREAD
-#define HM_JOIN_PER_THREAD 2  // queries a thread answers per step (measured: 2 beats 4 and 8)
+#define HM_JOIN_PER_THREAD 1  // queries a thread answers per step (measured: 1 beats 2, 4 and 8)
 #endif
 constexpr int kPerThread = HM_JOIN_PER_THREAD;
 constexpr int kRun = kThreads * kPerThread;  // queries a CTA answers per step

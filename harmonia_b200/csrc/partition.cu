@@ -156,6 +156,11 @@ __global__ void __launch_bounds__(1024) batch_chunk_kernel(BatchView bv, Chunk *
   }
 }
 
+#ifndef HM_PSA_HIST_PER
+#define HM_PSA_HIST_PER 8  // keys a histogram thread loads before counting them
+#endif
+constexpr int kHistPer = HM_PSA_HIST_PER;
+
 // Digit counts of one chunk per CTA.  whole_n >= 0: the input is one bucket
 // of whole_n queries cut into kChunk pieces, and this kernel writes that
 // chunk table itself (no chunk kernel before it).
@@ -195,15 +200,15 @@ __global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__res
   const int64_t *src = BATCHED ? cio[blockIdx.x].qbase : q;  // a chunk lies inside one batch
   for (int i = threadIdx.x; i < 256; i += kThreads) hist[i] = 0;
   __syncthreads();
-  for (int64_t base = c.begin; base < c.end; base += 8 * kThreads) {
-    int64_t k[8];
+  for (int64_t base = c.begin; base < c.end; base += kHistPer * kThreads) {
+    int64_t k[kHistPer];
 #pragma unroll
-    for (int j = 0; j < 8; j++) {  // all loads first
+    for (int j = 0; j < kHistPer; j++) {  // all loads first
       const int64_t i = base + j * kThreads + threadIdx.x;
       k[j] = i < c.end ? __ldg(src + i) : 0;
     }
 #pragma unroll
-    for (int j = 0; j < 8; j++)
+    for (int j = 0; j < kHistPer; j++)
       if (base + j * kThreads + threadIdx.x < c.end) atomicAdd(&hist[(bk(k[j]) >> shift2) & mask2], 1u);
   }
   __syncthreads();
