@@ -7,9 +7,11 @@
 // bucket, copies the bucket's leaf records (keys and values, 256 B per
 // 16-key leaf) from HBM into shared memory with 16-B loads in order, and
 // answers every query of the run from shared memory: a binary search over the
-// leaves' first keys picks the leaf, a scan of its keys the slot.  The leaf
-// range of each bucket comes from one descent per bucket boundary (a
-// separate kernel, one thread per boundary).  Leaves are read once per run
+// leaves' first keys (or, for batches of many queries per bucket, a 64-slot
+// directory of them built once per run) picks the leaf, a binary search of
+// its keys the slot.  The leaf range of each bucket comes from one descent per
+// bucket boundary (a separate kernel, one thread per boundary; kept per tree
+// shape between calls).  Leaves are read once per run
 // and sequentially, so the DRAM traffic of a batch with more queries than
 // leaves falls from a random 160 B per query to the size of the touched leaf
 // region.  A bucket whose leaves do not fit shared memory (very skewed keys)
