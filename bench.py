@@ -532,6 +532,38 @@ def main():
                                                        "cache_hints", "join")})
         del d_qs
 
+    # skewed point queries and ranges (the skewed + range workload): the
+    # tuned path on Zipf(0.99) queries, then 2^20 range queries with start
+    # uniform and length uniform in [1, 256], output compacted by prefix sum
+    if args.extras:
+        z = dg.gen_zipf_queries(sk, m, 0.99, seed=11)
+        d_z = torch.from_numpy(z).to(dev)
+        for _ in range(args.warmup):
+            tree.search(d_z, d_out)
+        z_ms = timed(args.steps, lambda: tree.search(d_z, d_out))
+        assert (d_out[:4096].cpu().numpy() == dg.values_for(z[:4096])).all(), "Zipf results are wrong"
+        del d_z
+        nr = 1 << 20
+        rs, rl = dg.gen_ranges(nr, 1, 256, seed=12)
+        d_rs, d_rl = torch.from_numpy(rs).to(dev), torch.from_numpy(rl.astype(np.int32)).to(dev)
+        for _ in range(args.warmup):
+            tree.range_search(d_rs, d_rl)
+        r_ms = timed(args.steps, lambda: tree.range_search(d_rs, d_rl))
+        off, rk, _ = tree.range_search(d_rs[:64], d_rl[:64])
+        i0 = np.searchsorted(sk, rs[:64])
+        exp_n = np.minimum(rl[:64].astype(np.int64), len(sk) - i0)
+        assert (np.diff(off.cpu().numpy()) == exp_n).all(), "range counts are wrong"
+        assert (rk[:int(exp_n[0])].cpu().numpy() == sk[i0[0]:i0[0] + exp_n[0]]).all(), "range keys are wrong"
+        records = int(np.minimum(rl.astype(np.int64), len(sk) - np.searchsorted(sk, rs)).sum())
+        extras["skewed_range"] = {
+            "zipf_point": {"value": round(ws * m / z_ms / 1e3, 1), "unit": UNIT, "ms_per_step": round(z_ms, 4),
+                           "what": "2^24 point queries, Zipf(0.99) over key rank, the tuned path"},
+            "range": {"value": round(ws * nr / r_ms / 1e3, 1), "unit": "Mranges/s", "ms_per_step": round(r_ms, 4),
+                      "records_per_s_m": round(ws * records / r_ms / 1e3, 1),
+                      "what": "2^20 ranges, start uniform, length uniform in [1, 256], compacted output "
+                              "(hm_range on device buffers, returns the total to the host)"}}
+        del d_rs, d_rl
+
     if args.extras:
         extras["batched_uneven"] = batched_uneven(tree, keys, sk, dev, timed, max(3, args.steps // 3),
                                                   args.warmup)
