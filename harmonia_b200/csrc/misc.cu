@@ -168,30 +168,62 @@ __global__ void range_locate_kernel(DevTree t, int f, int lc, int li, const int6
   }
 }
 
+// One warp per query.  The records of a query are the global ranks
+// [g0, g0 + count) in key order (g0 = leaf_base[first leaf] + first slot).
+// Per window of 32 leaves the warp loads their leaf_base entries (one
+// coalesced load); each lane finds the leaf of its record by a 5-step shuffle
+// search (the last leaf of the window whose base is <= the rank), so the
+// loads of all records are independent (no walk leaf by leaf).
 __global__ void range_copy_kernel(DevTree t, int lc, int li, const int32_t *__restrict__ first_leaf,
                                   const int32_t *__restrict__ first_slot,
                                   const int64_t *__restrict__ offsets, int64_t n,
                                   int64_t *__restrict__ okeys, int64_t *__restrict__ ovals) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + (threadIdx.x >> 5); i < n; i += warps) {
-    int64_t o = offsets[i];
-    int64_t rem = offsets[i + 1] - o;
-    int32_t leaf = first_leaf[i];
-    int slot = first_slot[i];
-    while (rem > 0 && leaf < t.n_leaf) {
-      int avail = __ldg(t.leaf_cnt + leaf) - slot;
-      int take = (int)(avail < rem ? avail : rem);
-      const int64_t *kr = t.leaf_rows + (int64_t)leaf * (li + 2 * lc) + li + slot;
-      const int64_t *vr = kr + lc;
-      for (int x = lane; x < take; x += 32) {
-        okeys[o + x] = __ldg(kr + x);
-        ovals[o + x] = __ldg(vr + x);
+  const int row = li + 2 * lc;
+  int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
+  // the next query's header is loaded while the current one is copied
+  int64_t o_n = 0, e_n = 0, L_n = 0, s_n = 0;
+  if (i < n) {
+    o_n = offsets[i];
+    e_n = offsets[i + 1];
+    L_n = first_leaf[i];
+    s_n = first_slot[i];
+  }
+  for (; i < n; i += warps) {
+    const int64_t o = o_n, rem = e_n - o_n, s0 = s_n;
+    int64_t L = L_n;
+    if (i + warps < n) {
+      o_n = offsets[i + warps];
+      e_n = offsets[i + warps + 1];
+      L_n = first_leaf[i + warps];
+      s_n = first_slot[i + warps];
+    }
+    if (rem <= 0) continue;  // uniform across the warp
+    const int64_t g0 = __ldg(t.leaf_base + L) + s0;
+    int64_t x0 = 0;
+    while (x0 < rem) {
+      const int64_t lb = L + lane < t.n_leaf ? __ldg(t.leaf_base + L + lane) : t.n_keys;
+      const int64_t wend = L + 32 < t.n_leaf ? __ldg(t.leaf_base + L + 32) : t.n_keys;
+      const int64_t xe = min(rem, wend - g0);  // this window holds records [x0, xe)
+      for (int64_t xb = x0; xb < xe; xb += 32) {
+        const int64_t x = xb + lane;
+        const int64_t r = g0 + x;
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int64_t v = __shfl_sync(0xffffffffu, lb, j + step);
+          if (v <= r) j += step;
+        }
+        const int64_t base = __shfl_sync(0xffffffffu, lb, j);
+        if (x < xe) {
+          const int64_t *kr = t.leaf_rows + (L + j) * row + li + (r - base);
+          okeys[o + x] = __ldg(kr);
+          ovals[o + x] = __ldg(kr + lc);
+        }
       }
-      o += take;
-      rem -= take;
-      leaf++;
-      slot = 0;
+      x0 = xe;
+      L += 32;
     }
   }
 }
