@@ -75,3 +75,31 @@ def test_empty_tree_and_empty_batch():
         assert off.tolist() == [0, 0, 0] and len(k) == 0
         off, k, v = t.range_search(np.zeros(0, np.int64), np.zeros(0, np.int32))
         assert off.tolist() == [0]
+
+
+@pytest.mark.parametrize("leaf_cap,fill", [(16, 1), (16, 3), (64, 5)])
+def test_ranges_across_many_sparse_leaves(leaf_cap, fill):
+    # a few keys per leaf: one range spans up to 256 leaves, so the copy walks
+    # several 32-leaf windows of leaf_base, with ranges starting and ending
+    # anywhere inside them and running past the last key
+    keys = dg.gen_keys(20000, seed=31)
+    sk = np.sort(keys)
+    sv = dg.values_for(sk)
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), leaf_cap=leaf_cap, leaf_fill=fill) as t:
+        st, ln = dg.gen_ranges(3000, 1, 256, seed=32)
+        st[:40] = sk[np.arange(40) * 400]   # exact key starts
+        st[40:48] = sk[-8:]                 # near the end: the copy stops at the last key
+        ln[:48] = 256
+        oracle = po.PortTree(sk, sv)
+        got = t.range_search(cuda(st), cuda(ln))
+        exp = oracle.range(st, ln)
+        for a, b in zip(got, exp):
+            assert (a.cpu().numpy() == b).all()
+        # after deletes leave leaves of uneven size (none empty)
+        gone = sk[5:20000:3]
+        t.delete(gone)
+        ek = np.setdiff1d(sk, gone)
+        got = t.range_search(cuda(st), cuda(ln))
+        exp = po.PortTree(ek, dg.values_for(ek)).range(st, ln)
+        for a, b in zip(got, exp):
+            assert (a.cpu().numpy() == b).all()
