@@ -7,6 +7,8 @@
 // difference in a report is the layout and the search, not the data.
 #include "hm_internal.cuh"
 
+#include <mutex>
+
 #include <algorithm>
 
 namespace hm {
@@ -88,10 +90,18 @@ extern "C" int hm_search_baseline(hm_tree *t, int kind, const int64_t *q, size_t
   if (n == 0) return HM_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(hs);
   const int f = t->cfg.fanout;
-  if (!t->child_ids || t->child_ids_generation != t->generation) {
+  // The child ids are built once per arena, under the tree's lock; a caller on
+  // another stream that finds them built waits for the build's event.
+  std::unique_lock<std::mutex> lk(t->mu);
+  if (t->child_ids && t->child_ids_generation == t->generation) {
+    cudaError_t e = cudaStreamWaitEvent(s, t->child_ids_ready, 0);
+    if (e != cudaSuccess) return cuda_err(e);
+  } else {
     if (t->child_ids) cudaFree(t->child_ids);
     t->child_ids = nullptr;
-    cudaError_t e = cudaMalloc(&t->child_ids, (size_t)std::max<int64_t>(t->n_inner * f, 1) * 4);
+    cudaError_t e = cudaSuccess;
+    if (!t->child_ids_ready) e = cudaEventCreateWithFlags(&t->child_ids_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&t->child_ids, (size_t)std::max<int64_t>(t->n_inner * f, 1) * 4);
     if (e != cudaSuccess) {
       t->child_ids = nullptr;
       return cuda_err(e);
@@ -105,8 +115,15 @@ extern "C" int hm_search_baseline(hm_tree *t, int kind, const int64_t *q, size_t
     const unsigned grid = (unsigned)std::min<int64_t>((total + kThreads - 1) / kThreads + 1, 148 * 32);
     child_ids_kernel<<<grid, kThreads, 0, s>>>(t->prefix, lv, f, t->child_ids);
     note_launch();
+    e = cudaEventRecord(t->child_ids_ready, s);
+    if (e != cudaSuccess) {
+      cudaFree(t->child_ids);
+      t->child_ids = nullptr;
+      return cuda_err(e);
+    }
     t->child_ids_generation = t->generation;
   }
+  lk.unlock();
   const unsigned grid = (unsigned)std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)t->num_sms * 8);
   pointer_search_kernel<<<grid, kThreads, 0, s>>>(t->inner, t->child_ids, t->leaf_rows, t->height, t->n_inner, f,
                                                   t->cfg.leaf_cap, t->leaf_index, q, n, out);

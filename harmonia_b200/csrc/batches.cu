@@ -201,9 +201,10 @@ int hm_search_batches(hm_tree *t, const hm_batch *batches, int nb, hm_stream hs)
   if (rc) return rc;
   const SearchPlan plan = plan_search(t, total, nb);
   const size_t set_bytes = img.size();
-  rc = ensure_scratch(t, set_bytes + batches_work_bytes(t, total, plan));
+  ScratchLease lease(t, s);
+  rc = lease.acquire(set_bytes + batches_work_bytes(t, total, plan));
   if (rc) return rc;
-  char *d = static_cast<char *>(t->scratch);
+  char *d = static_cast<char *>(lease.ptr());
   cudaError_t e = cudaMemcpyAsync(d, img.data(), set_bytes, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return cuda_err(e);
   int tok = prof_begin(t, s);

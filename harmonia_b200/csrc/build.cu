@@ -152,9 +152,10 @@ void check_sorted_keys(const uint64_t *ukeys, int64_t n, unsigned *d_flags, cuda
   note_launch();
 }
 
-int build_from_sorted(hm_tree *t, const uint64_t *ukeys, const int64_t *vals, int64_t n,
+int build_from_sorted(const BuildTarget &b, const uint64_t *ukeys, const int64_t *vals, int64_t n,
                       int64_t *tmp_a, int64_t *tmp_b, cudaStream_t s) {
-  const int lc = t->cfg.leaf_cap, f = t->cfg.fanout;
+  const BuildTarget *t = &b;
+  const int lc = t->leaf_cap, f = t->fanout;
   int64_t leaf_words = t->n_leaf * (int64_t)t->leaf_row;
   leaf_kernel<<<min(blocks_for(leaf_words), 148u * 32), kThreads, 0, s>>>(
       ukeys, vals, n, t->n_leaf, lc, t->leaf_index, t->leaf_rows, t->leaf_cnt, t->leaf_base, tmp_a);

@@ -36,23 +36,92 @@ int cuda_err(cudaError_t e) {
   return HM_ECUDA;
 }
 
-int ensure_scratch(hm_tree *t, size_t bytes) {
-  if (bytes <= t->scratch_bytes) return HM_OK;
-  if (t->scratch) {
-    cudaError_t e = cudaDeviceSynchronize();
+// Idle blocks kept per tree before a busy stream's block is reused instead of
+// adding one (each holds as much as its largest call needed).
+constexpr size_t kPoolBlocks = 8;
+
+int ScratchLease::acquire(size_t bytes) {
+  if (idx_ >= 0) return HM_EINVAL;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s_, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return HM_EINVAL;
+  }
+  if (cs != cudaStreamCaptureStatusNone) return HM_EINVAL;
+  std::lock_guard<std::mutex> lk(t_->mu);
+  auto &pool = t_->pool;
+  int pick = -1;
+  for (size_t i = 0; i < pool.size() && pick < 0; i++)  // last used on this stream
+    if (!pool[i].leased && pool[i].stream == s_) pick = (int)i;
+  for (size_t i = 0; i < pool.size() && pick < 0; i++) {  // last use finished
+    if (pool[i].leased) continue;
+    if (!pool[i].recorded) {
+      pick = (int)i;
+    } else {
+      const cudaError_t q = cudaEventQuery(pool[i].done);
+      if (q == cudaSuccess) pick = (int)i;
+      else cudaGetLastError();  // not ready (or an earlier failure reported elsewhere)
+    }
+  }
+  bool any_idle = false;
+  for (auto &b : pool) any_idle |= !b.leased;
+  if (pick < 0 && (pool.size() < kPoolBlocks || !any_idle)) {  // a new block
+    hm_tree::ScratchBlock b;
+    cudaError_t e = cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_err(e);
-    cudaFree(t->scratch);
-    t->scratch = nullptr;
-    t->scratch_bytes = 0;
+    pool.push_back(b);
+    pick = (int)pool.size() - 1;
   }
-  size_t want = (size_t)align_up((int64_t)bytes, 1 << 20);
-  cudaError_t e = cudaMalloc(&t->scratch, want);
-  if (e != cudaSuccess) {
-    t->scratch = nullptr;
-    return cuda_err(e);
+  if (pick < 0) {  // the block idle longest; s waits for its last use
+    for (size_t i = 0; i < pool.size(); i++)
+      if (!pool[i].leased && (pick < 0 || pool[i].tick < pool[pick].tick)) pick = (int)i;
   }
-  t->scratch_bytes = want;
+  hm_tree::ScratchBlock &b = pool[pick];
+  if (b.recorded) {
+    cudaError_t e = cudaStreamWaitEvent(s_, b.done, 0);
+    if (e != cudaSuccess) return cuda_err(e);
+  }
+  if (b.bytes < bytes) {
+    if (b.ptr) cudaFreeAsync(b.ptr, s_);  // after the block's previous use, in stream order
+    b.ptr = nullptr;
+    b.bytes = 0;
+    const size_t want = (size_t)align_up((int64_t)bytes, 1 << 20);
+    cudaError_t e = cudaMallocAsync(&b.ptr, want, s_);
+    if (e != cudaSuccess) {
+      b.ptr = nullptr;
+      return cuda_err(e);
+    }
+    b.bytes = want;
+  }
+  b.stream = s_;
+  b.leased = true;
+  idx_ = pick;
   return HM_OK;
+}
+
+ScratchLease::~ScratchLease() {
+  if (idx_ < 0) return;
+  std::lock_guard<std::mutex> lk(t_->mu);
+  hm_tree::ScratchBlock &b = t_->pool[idx_];
+  if (cudaEventRecord(b.done, s_) == cudaSuccess) {
+    b.recorded = true;
+  } else {
+    cudaGetLastError();
+  }
+  b.leased = false;
+  b.tick = ++t_->pool_tick;
+}
+
+void *ScratchLease::ptr() const { return idx_ < 0 ? nullptr : t_->pool[idx_].ptr; }
+size_t ScratchLease::bytes() const { return idx_ < 0 ? 0 : t_->pool[idx_].bytes; }
+
+void free_scratch_pool(hm_tree *t) {
+  for (auto &b : t->pool) {
+    if (b.ptr) cudaFreeAsync(b.ptr, 0);
+    if (b.done) cudaEventDestroy(b.done);
+  }
+  t->pool.clear();
+  cudaStreamSynchronize(0);
 }
 
 static const char *kStageNames[kStageCount] = {"partition", "search", "search_batches", "range",
@@ -71,6 +140,7 @@ static cudaEvent_t prof_event(hm_tree *t) {
 
 int prof_begin(hm_tree *t, cudaStream_t s) {
   if (!t->prof) return -1;
+  std::lock_guard<std::mutex> lk(t->mu);
   hm_tree::ProfRec r{-1, prof_event(t), prof_event(t)};
   cudaEventRecord(r.a, s);
   t->prof_recs.push_back(r);
@@ -78,7 +148,9 @@ int prof_begin(hm_tree *t, cudaStream_t s) {
 }
 
 void prof_end(hm_tree *t, int stage, int token, cudaStream_t s) {
-  if (token < 0 || token >= (int)t->prof_recs.size()) return;
+  if (token < 0) return;
+  std::lock_guard<std::mutex> lk(t->mu);
+  if (token >= (int)t->prof_recs.size()) return;
   t->prof_recs[token].stage = stage;
   cudaEventRecord(t->prof_recs[token].b, s);
 }
@@ -196,7 +268,8 @@ int free_tree(hm_tree *t) {
   if (t->child_ids) cudaFree(t->child_ids);
   if (t->join_leafb) cudaFree(t->join_leafb);
   if (t->join_leafb_ready) cudaEventDestroy(t->join_leafb_ready);
-  if (t->scratch) cudaFree(t->scratch);
+  if (t->child_ids_ready) cudaEventDestroy(t->child_ids_ready);
+  free_scratch_pool(t);
   if (t->d_err) cudaFree(t->d_err);
   if (t->pinned) cudaFreeHost(t->pinned);
   for (auto &s : t->io_stream)
@@ -469,7 +542,7 @@ int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_c
     if (e != cudaSuccess) return cuda_err(e);
     return (hflags & 2u) ? HM_EMAXKEY : HM_EDUPLICATE;
   }
-  rc = build_from_sorted(t, uk, vv, n, reinterpret_cast<int64_t *>(uk_alt), vv_alt, s);
+  rc = build_from_sorted(t->target(), uk, vv, n, reinterpret_cast<int64_t *>(uk_alt), vv_alt, s);
   if (rc == HM_OK && n > 0) {
     uint64_t ends[2] = {0, 0};
     cudaMemcpyAsync(&ends[0], uk, 8, cudaMemcpyDeviceToHost, s);
@@ -546,13 +619,19 @@ int hm_search(hm_tree *t, const int64_t *q, size_t n_, int64_t *out, hm_stream h
   cudaStream_t s = as_stream(hs);
   bool dq = is_device_ptr(q), dout = is_device_ptr(out);
   if (dq && dout) {
-    int rc = ensure_scratch(t, search_scratch_need(t, n));
-    if (rc) return rc;
-    return search_device(t, q, n, out, s, t->scratch, t->scratch_bytes);
+    const size_t need = search_scratch_need(t, n);
+    ScratchLease lease(t, s);
+    if (need > 0) {
+      int rc = lease.acquire(need);
+      if (rc) return rc;
+    }
+    return search_device(t, q, n, out, s, lease.ptr(), lease.bytes());
   }
   if (dq != dout) return HM_EINVAL;  // mixed host/device buffers are not supported
   // Host buffers: chunked pipeline over a ring of kIoRing device buffers, copies
   // in and out on their own streams overlapping the search of other chunks.
+  // One host-buffer search at a time per tree (copy streams, events, staging).
+  std::lock_guard<std::mutex> io_lock(t->io_mu);
   int rc = ensure_io(t);
   if (rc) return rc;
   constexpr int R = kIoRing;
@@ -564,9 +643,10 @@ int hm_search(hm_tree *t, const int64_t *q, size_t n_, int64_t *out, hm_stream h
     sneed = std::max(sneed, search_scratch_need(t, m));
   }
   const size_t cbytes = (size_t)align_up(chunk * 8, 256);
-  rc = ensure_scratch(t, 2 * R * cbytes + sneed);
+  ScratchLease lease(t, s);  // its previous use is ordered before s, which the pipeline waits for
+  rc = lease.acquire(2 * R * cbytes + sneed);
   if (rc) return rc;
-  char *sb = static_cast<char *>(t->scratch);
+  char *sb = static_cast<char *>(lease.ptr());
   int64_t *dqb[R], *dob[R];
   for (int b = 0; b < R; b++) {
     dqb[b] = reinterpret_cast<int64_t *>(sb + (size_t)b * cbytes);
@@ -643,11 +723,15 @@ int hm_sync(hm_tree *t, hm_stream hs) {
   if (!t) return HM_EINVAL;
   cudaError_t e = cudaStreamSynchronize(as_stream(hs));
   if (e != cudaSuccess) return cuda_err(e);
+  // the error word is read on the caller's stream (the legacy default stream
+  // would also wait for other streams' work on this device)
   unsigned err = 0;
-  e = cudaMemcpy(&err, t->d_err, 4, cudaMemcpyDeviceToHost);
+  e = cudaMemcpyAsync(&err, t->d_err, 4, cudaMemcpyDeviceToHost, as_stream(hs));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(hs));
   if (e != cudaSuccess) return cuda_err(e);
   if (err) {
-    cudaMemset(t->d_err, 0, 4);
+    cudaMemsetAsync(t->d_err, 0, 4, as_stream(hs));
+    cudaStreamSynchronize(as_stream(hs));
     return (err & kErrTimeout) ? HM_ETIMEOUT : HM_ECUDA;
   }
   return HM_OK;
@@ -666,10 +750,11 @@ int hm_export(hm_tree *t, int64_t *keys, int64_t *vals, size_t cap, size_t *n) {
     return cuda_err(cudaStreamSynchronize(s));
   }
   const size_t b = (size_t)align_up(t->n_keys * 8, 256);
-  int rc = ensure_scratch(t, 2 * b);
+  ScratchLease lease(t, s);
+  int rc = lease.acquire(2 * b);
   if (rc) return rc;
-  int64_t *ek = static_cast<int64_t *>(t->scratch);
-  int64_t *ev = reinterpret_cast<int64_t *>(static_cast<char *>(t->scratch) + b);
+  int64_t *ek = static_cast<int64_t *>(lease.ptr());
+  int64_t *ev = reinterpret_cast<int64_t *>(static_cast<char *>(lease.ptr()) + b);
   export_contents(t, ek, ev, s);
   cudaError_t e = cudaMemcpyAsync(keys, ek, t->n_keys * 8, cudaMemcpyDefault, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(vals, ev, t->n_keys * 8, cudaMemcpyDefault, s);
@@ -677,21 +762,29 @@ int hm_export(hm_tree *t, int64_t *keys, int64_t *vals, size_t cap, size_t *n) {
   return cuda_err(e);
 }
 
-int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n_, int64_t *offsets,
-             int64_t *okeys, int64_t *ovals, size_t cap, size_t *total, hm_stream hs) {
-  if (!t || (n_ > 0 && (!start || !len)) || !offsets) return HM_EINVAL;
+}  // extern "C"
+
+namespace {
+
+// Body of hm_range (len given, end == nullptr) and hm_range_between (end
+// given, len == nullptr): locate, scan of the counts into offsets, total to
+// the host, compacted copy.
+int range_impl(hm_tree *t, const int64_t *start, const int32_t *len, const int64_t *end, size_t n_,
+               int64_t *offsets, int64_t *okeys, int64_t *ovals, size_t cap, size_t *total, hm_stream hs) {
   const int64_t n = (int64_t)n_;
   cudaStream_t s = as_stream(hs);
   if (total) *total = 0;
-  const bool dev_in = n == 0 || (is_device_ptr(start) && is_device_ptr(len));
+  const void *second = end ? static_cast<const void *>(end) : static_cast<const void *>(len);
+  const bool dev_in = n == 0 || (is_device_ptr(start) && is_device_ptr(second));
   const bool dev_out = is_device_ptr(offsets);
   const size_t b8 = (size_t)align_up((n + 1) * 8, 256), b4 = (size_t)align_up(n * 4 + 4, 256);
   size_t need = 2 * b4 + b8 + (size_t)align_up((int64_t)scan_scratch_bytes(n + 1), 256);
-  if (!dev_in) need += b8 + b4;
+  if (!dev_in) need += b8 + (end ? b8 : b4);
   if (!dev_out) need += b8;
-  int rc = ensure_scratch(t, need);
+  ScratchLease lease(t, s);
+  int rc = lease.acquire(need);
   if (rc) return rc;
-  char *p = static_cast<char *>(t->scratch);
+  char *p = static_cast<char *>(lease.ptr());
   int32_t *fl = reinterpret_cast<int32_t *>(p);
   p += b4;
   int32_t *fs = reinterpret_cast<int32_t *>(p);
@@ -702,22 +795,30 @@ int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n_, in
   p += align_up((int64_t)scan_scratch_bytes(n + 1), 256);
   const int64_t *d_start = start;
   const int32_t *d_len = len;
+  const int64_t *d_end = end;
   cudaError_t e = cudaSuccess;
   if (!dev_in) {
     int64_t *ds = reinterpret_cast<int64_t *>(p);
     p += b8;
-    int32_t *dl = reinterpret_cast<int32_t *>(p);
-    p += b4;
     e = cudaMemcpyAsync(ds, start, n * 8, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dl, len, n * 4, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return cuda_err(e);
     d_start = ds;
-    d_len = dl;
+    if (end) {
+      int64_t *de = reinterpret_cast<int64_t *>(p);
+      p += b8;
+      if (e == cudaSuccess) e = cudaMemcpyAsync(de, end, n * 8, cudaMemcpyHostToDevice, s);
+      d_end = de;
+    } else {
+      int32_t *dl = reinterpret_cast<int32_t *>(p);
+      p += b4;
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dl, len, n * 4, cudaMemcpyHostToDevice, s);
+      d_len = dl;
+    }
+    if (e != cudaSuccess) return cuda_err(e);
   }
   int64_t *d_off = dev_out ? offsets : reinterpret_cast<int64_t *>(p);
   const int tok = prof_begin(t, s);
   if (n > 0) {
-    rc = range_locate(t, d_start, d_len, n, fl, fs, cnt, s);
+    rc = range_locate(t, d_start, d_len, d_end, n, fl, fs, cnt, s);
     if (rc) return rc;
   }
   exclusive_scan_i64(cnt, d_off, n, scan_scratch, s);
@@ -727,7 +828,8 @@ int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n_, in
   if (e != cudaSuccess) return cuda_err(e);
   if (total) *total = (size_t)tot;
   if (!dev_out) {
-    e = cudaMemcpy(offsets, d_off, (n + 1) * 8, cudaMemcpyDeviceToHost);
+    e = cudaMemcpyAsync(offsets, d_off, (n + 1) * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_err(e);
   }
   if ((size_t)tot > cap) return HM_ECAPACITY;
@@ -740,8 +842,10 @@ int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n_, in
     if (rc) return rc;
     return hm_sync(t, hs);
   }
+  // host record buffers: a stream-ordered temporary (no device-wide
+  // synchronisation, unlike cudaMalloc/cudaFree)
   int64_t *tk = nullptr;
-  e = cudaMalloc(&tk, 2 * (size_t)align_up(tot * 8, 256));
+  e = cudaMallocAsync(reinterpret_cast<void **>(&tk), 2 * (size_t)align_up(tot * 8, 256), s);
   if (e != cudaSuccess) return cuda_err(e);
   int64_t *tv = reinterpret_cast<int64_t *>(reinterpret_cast<char *>(tk) + align_up(tot * 8, 256));
   rc = range_copy_out(t, fl, fs, d_off, n, tk, tv, s);
@@ -749,11 +853,29 @@ int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n_, in
   if (rc == HM_OK) {
     e = cudaMemcpyAsync(okeys, tk, tot * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ovals, tv, tot * 8, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    rc = cuda_err(e);
   }
-  cudaFree(tk);
+  cudaFreeAsync(tk, s);
+  if (rc == HM_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (rc == HM_OK) rc = cuda_err(e);
   return rc ? rc : hm_sync(t, hs);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n, int64_t *offsets,
+             int64_t *okeys, int64_t *ovals, size_t cap, size_t *total, hm_stream hs) {
+  if (total) *total = 0;
+  if (!t || (n > 0 && (!start || !len)) || !offsets) return HM_EINVAL;
+  return range_impl(t, start, len, nullptr, n, offsets, okeys, ovals, cap, total, hs);
+}
+
+int hm_range_between(hm_tree *t, const int64_t *start, const int64_t *end, size_t n, int64_t *offsets,
+                     int64_t *okeys, int64_t *ovals, size_t cap, size_t *total, hm_stream hs) {
+  if (total) *total = 0;
+  if (!t || (n > 0 && (!start || !end)) || !offsets) return HM_EINVAL;
+  return range_impl(t, start, nullptr, end, n, offsets, okeys, ovals, cap, total, hs);
 }
 
 int hm_delete_batch(hm_tree *t, const int64_t *keys, size_t n_, size_t *removed, hm_stream hs) {
@@ -858,12 +980,14 @@ int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n_, hm_config *best)
   for (const hm_config &c : cands) {
     t->cfg = c;
     choose_smem_levels(t);
-    rc = ensure_scratch(t, search_scratch_need(t, n));
+    ScratchLease lease(t, 0);
+    const size_t need = search_scratch_need(t, n);
+    if (need > 0) rc = lease.acquire(need);
     if (rc) break;
     float ms = 1e30f;
     for (int rep = 0; rep < 3 && rc == HM_OK; rep++) {
       cudaEventRecord(a, 0);
-      rc = search_device(t, sample_q, n, d_out, 0, t->scratch, t->scratch_bytes);
+      rc = search_device(t, sample_q, n, d_out, 0, lease.ptr(), lease.bytes());
       cudaEventRecord(b, 0);
       cudaEventSynchronize(b);
       float x = 0;
@@ -906,7 +1030,13 @@ int hm_profile_read(hm_tree *t, hm_stage_time *out, int cap, int *n) {
   double ms[kStageCount] = {};
   uint64_t cnt[kStageCount] = {};
   int rc = HM_OK;
-  for (auto &r : t->prof_recs) {
+  std::vector<hm_tree::ProfRec> recs;
+  {
+    std::lock_guard<std::mutex> lk(t->mu);
+    recs.swap(t->prof_recs);
+  }
+  std::vector<cudaEvent_t> back;
+  for (auto &r : recs) {
     if (r.stage >= 0) {
       cudaError_t e = cudaEventSynchronize(r.b);
       float x = 0;
@@ -915,10 +1045,13 @@ int hm_profile_read(hm_tree *t, hm_stage_time *out, int cap, int *n) {
       ms[r.stage] += x;
       cnt[r.stage]++;
     }
-    t->prof_pool.push_back(r.a);
-    t->prof_pool.push_back(r.b);
+    back.push_back(r.a);
+    back.push_back(r.b);
   }
-  t->prof_recs.clear();
+  {
+    std::lock_guard<std::mutex> lk(t->mu);
+    t->prof_pool.insert(t->prof_pool.end(), back.begin(), back.end());
+  }
   int k = 0;
   for (int i = 0; i < kStageCount; i++) {
     if (!cnt[i]) continue;

@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -98,6 +99,20 @@ __host__ __device__ inline int64_t part_start(int64_t j, int64_t total, int64_t 
 
 inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
+// The shape and arrays a bulk build writes: a tree's own arena, or a new one
+// being built for a rebuild before it is swapped in.
+struct BuildTarget {
+  int fanout = 0, leaf_cap = 0;
+  int height = 0, inner_row = 0, leaf_row = 0, leaf_index = 0;
+  int64_t n_inner = 0, n_leaf = 0;
+  int64_t lvl_start[kMaxLevels + 1] = {};
+  int64_t *inner = nullptr;
+  int32_t *prefix = nullptr;
+  int64_t *leaf_rows = nullptr;
+  int32_t *leaf_cnt = nullptr;
+  int64_t *leaf_base = nullptr;
+};
+
 // Counts kernel launches issued by this library (hm_launch_count); launches
 // recorded into a CUDA graph are counted when the graph is replayed.
 void note_launch(int n = 1);
@@ -129,9 +144,11 @@ struct hm_tree {
   mutable int join_leafb_bits = 0;
   mutable cudaEvent_t join_leafb_ready = nullptr;
   int64_t join_tuned_min = INT64_MAX;  // smallest batch the autotuner saw the join win
-  // comparison baseline (hm_search_baseline): children ids per inner node
+  // comparison baseline (hm_search_baseline): children ids per inner node,
+  // child_ids_ready recorded after the kernel that filled them
   int32_t *child_ids = nullptr;
   uint64_t child_ids_generation = ~0ull;
+  cudaEvent_t child_ids_ready = nullptr;
   // arena
   void *arena = nullptr;
   size_t arena_bytes = 0;
@@ -140,9 +157,30 @@ struct hm_tree {
   int64_t *leaf_rows = nullptr;
   int32_t *leaf_cnt = nullptr;
   int64_t *leaf_base = nullptr;
-  // per-tree scratch (grown on demand), error word, pinned staging
-  void *scratch = nullptr;
-  size_t scratch_bytes = 0;
+  // Scratch pool: blocks of working memory leased to one call at a time
+  // (ScratchLease).  A block is ordered on the device after its previous use
+  // by the event recorded at the end of that use, so reads enqueued on
+  // different streams (or from different host threads) never share a block
+  // while either runs, and a block grows with a stream-ordered free and
+  // allocation instead of a device-wide synchronisation.
+  struct ScratchBlock {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaStream_t stream = nullptr;  // stream of the last use
+    cudaEvent_t done = nullptr;     // recorded at the end of the last use
+    bool recorded = false;
+    bool leased = false;
+    uint64_t tick = 0;  // release order, for reuse of the block idle longest
+  };
+  std::vector<ScratchBlock> pool;
+  uint64_t pool_tick = 0;
+  // guards the host-side state that concurrent calls share: the scratch pool,
+  // the join boundary cache, the comparison kernel's child ids and the
+  // profiling records
+  mutable std::mutex mu;
+  // held for a whole host-buffer search: its copy streams, events and pinned
+  // staging serve one call at a time
+  std::mutex io_mu;
   unsigned *d_err = nullptr;
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -156,6 +194,25 @@ struct hm_tree {
   bool prof = false;
   std::vector<ProfRec> prof_recs;
   std::vector<cudaEvent_t> prof_pool;
+
+  hm::BuildTarget target() const {
+    hm::BuildTarget b;
+    b.fanout = cfg.fanout;
+    b.leaf_cap = cfg.leaf_cap;
+    b.height = height;
+    b.inner_row = inner_row;
+    b.leaf_row = leaf_row;
+    b.leaf_index = leaf_index;
+    b.n_inner = n_inner;
+    b.n_leaf = n_leaf;
+    for (int i = 0; i <= hm::kMaxLevels; i++) b.lvl_start[i] = lvl_start[i];
+    b.inner = inner;
+    b.prefix = prefix;
+    b.leaf_rows = leaf_rows;
+    b.leaf_cnt = leaf_cnt;
+    b.leaf_base = leaf_base;
+    return b;
+  }
 
   hm::DevTree view() const {
     hm::DevTree d;
@@ -225,9 +282,9 @@ bool radix_sort_pairs(uint64_t *ukeys, V *vals, uint64_t *ukeys_alt, V *vals_alt
 // ---- bulk build (build.cu) ----
 int shape(int64_t n, const hm_config &c, int *height, int64_t *lvl_start,
           int64_t *n_inner, int64_t *n_leaf);
-// Builds the tree arrays of t (already sized and allocated) from sorted
-// unsigned-transformed keys; writes flags (bit0 dup, bit1 maxkey) to d_flags.
-int build_from_sorted(hm_tree *t, const uint64_t *ukeys, const int64_t *vals,
+// Builds the arrays of b (already sized and allocated) from sorted
+// unsigned-transformed keys.
+int build_from_sorted(const BuildTarget &b, const uint64_t *ukeys, const int64_t *vals,
                       int64_t n, int64_t *tmp_a, int64_t *tmp_b, cudaStream_t s);
 void check_sorted_keys(const uint64_t *ukeys, int64_t n, unsigned *d_flags, cudaStream_t s);
 void transform_keys_in(const int64_t *keys, uint64_t *ukeys, int64_t n, cudaStream_t s);
@@ -285,7 +342,9 @@ void exclusive_scan_i64(const int64_t *in, int64_t *out, int64_t n, void *scratc
 void exclusive_scan_i32(const int32_t *in, int64_t *out, int64_t n, void *scratch, cudaStream_t s);
 void export_contents(const hm_tree *t, int64_t *d_keys, int64_t *d_vals, cudaStream_t s);
 size_t range_scratch_bytes(int64_t n);
-int range_locate(const hm_tree *t, const int64_t *start, const int32_t *len, int64_t n,
+// Counts per query: the first len[i] records >= start[i] (end == nullptr), or
+// every record in [start[i], end[i]] (len unused).
+int range_locate(const hm_tree *t, const int64_t *start, const int32_t *len, const int64_t *end, int64_t n,
                  int32_t *first_leaf, int32_t *first_slot, int64_t *count, cudaStream_t s);
 int range_copy_out(const hm_tree *t, const int32_t *first_leaf, const int32_t *first_slot,
                    const int64_t *offsets, int64_t n, int64_t *okeys, int64_t *ovals, cudaStream_t s);
@@ -337,8 +396,33 @@ int run_search(hm_tree *t, const int64_t *d_q, int64_t n, int64_t *d_out, cudaSt
 size_t run_search_scratch(const hm_tree *t, int64_t n);
 void refresh_smem_levels(hm_tree *t);
 
+// ---- scratch pool (harmonia.cu) ----
+// A lease on one block of t's scratch pool for the work one call enqueues on
+// stream s.  acquire(bytes) picks an idle block (the one last used on s, else
+// one whose last use has finished, else a new one while the pool is small,
+// else the one idle longest), makes s wait for the block's previous use and
+// grows it on s if needed.  The destructor records the end of this use on s
+// and returns the block to the pool, so the caller must have enqueued all
+// work that touches the block by then.  A stream under graph capture gets
+// HM_EINVAL: captured work uses memory the graph owns (hm_plan_create).
+class ScratchLease {
+ public:
+  ScratchLease(hm_tree *t, cudaStream_t s) : t_(t), s_(s) {}
+  ~ScratchLease();
+  ScratchLease(const ScratchLease &) = delete;
+  ScratchLease &operator=(const ScratchLease &) = delete;
+  int acquire(size_t bytes);
+  void *ptr() const;
+  size_t bytes() const;
+
+ private:
+  hm_tree *t_;
+  cudaStream_t s_;
+  int idx_ = -1;
+};
+void free_scratch_pool(hm_tree *t);  // after the device is idle
+
 // ---- misc ----
-int ensure_scratch(hm_tree *t, size_t bytes);
 int cuda_err(cudaError_t e);
 
 }  // namespace hm

@@ -24,6 +24,8 @@
 // range whose first key is <= q is the leaf the descent would reach.
 #include "hm_internal.cuh"
 
+#include <mutex>
+
 #include <algorithm>
 
 namespace hm {
@@ -414,7 +416,12 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
   }
   bool want_leafb = true;
   bool fill_cache = false;
+  // Held until the fill (if any) is enqueued and its event recorded: another
+  // caller then finds the cache valid and waits on that event.  Once filled
+  // the cache is only read, until a write to the tree changes its shape.
+  std::unique_lock<std::mutex> cache_lock(t->mu, std::defer_lock);
   if (cap == cudaStreamCaptureStatusNone) {
+    cache_lock.lock();
     const bool same = t->join_leafb_valid && t->join_leafb_gen == t->generation &&
                       t->join_leafb_shape == t->shape_version && t->join_leafb_lo == t->key_min &&
                       t->join_leafb_hi == t->key_max && t->join_leafb_nleaf == t->n_leaf && t->join_leafb_bits == bits;
@@ -453,6 +460,7 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
     t->join_leafb_nleaf = t->n_leaf;
     t->join_leafb_bits = bits;
   }
+  if (cache_lock.owns_lock()) cache_lock.unlock();
   exclusive_scan_i32(cnt, first, nb + 1, scan, s);
   launch_pdl(expand_items_kernel, gb, 256, 0, s, nb, bstart, leafb, cnt, first, items);
   const int lc = t->cfg.leaf_cap;

@@ -5,8 +5,9 @@
 // (open-harmonia/src/range.cu:101-227) descends with the start key and copies
 // up to Range_Size = 8 records into fixed per-query slots (no compaction),
 // with the end key forced to Max_Key (open-harmonia/src/range.cu:349-355).
-// Here a query asks for the first len[i] records with key >= start[i]; a
-// locate pass descends and computes each query's count, an exclusive scan
+// Here a query asks for the first len[i] records with key >= start[i], or
+// (inclusive form) every record with start[i] <= key <= end[i]; a locate pass
+// descends and computes each query's count, an exclusive scan
 // turns counts into offsets, and a copy pass (one warp per query) writes the
 // records contiguously: leaves are ordered, so the records of a query are the
 // key-ordered run that starts at (leaf, slot) and continues in leaf+1, ...
@@ -141,15 +142,25 @@ __global__ void export_kernel(DevTree t, int lc, int li, int64_t *__restrict__ k
   }
 }
 
+// One thread per query: descend with the start key, take its lower bound in
+// the leaf (global rank g through leaf_base).  Length form (end == nullptr):
+// count = min(len, keys from g to the end).  Inclusive form: a second descent
+// with the end key gives the global rank of its upper bound (keys <= end: the
+// leaves before the end key's leaf hold only smaller keys, the ones after only
+// larger, because separators fence the leaves), count = that rank - g, and
+// nothing when end < start (BPlusTree::range_search,
+// open-harmonia/src/bpt.cpp:695-769).  The end key Max_Key reaches the end of
+// the key space without a descent.
 __global__ void range_locate_kernel(DevTree t, int f, int lc, int li, const int64_t *__restrict__ start,
-                                    const int32_t *__restrict__ len, int64_t n,
-                                    int32_t *__restrict__ first_leaf, int32_t *__restrict__ first_slot,
-                                    int64_t *__restrict__ count) {
+                                    const int32_t *__restrict__ len, const int64_t *__restrict__ end,
+                                    int64_t n, int32_t *__restrict__ first_leaf,
+                                    int32_t *__restrict__ first_slot, int64_t *__restrict__ count) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t s = __ldg(start + i);
-    int64_t want = __ldg(len + i);
-    if (want <= 0 || s == kMaxKey || t.n_keys == 0) {
+    const int64_t s = __ldg(start + i);
+    const int64_t e = end ? __ldg(end + i) : 0;
+    const bool empty = end ? (e < s) : (__ldg(len + i) <= 0);
+    if (empty || s == kMaxKey || t.n_keys == 0) {
       first_leaf[i] = 0;
       first_slot[i] = 0;
       count[i] = 0;
@@ -161,10 +172,23 @@ __global__ void range_locate_kernel(DevTree t, int f, int lc, int li, const int6
     int lb = 0;  // first slot with key >= start
     while (lb < cnt && __ldg(kr + lb) < s) lb++;
     int64_t g = __ldg(t.leaf_base + leaf) + lb;
-    int64_t rem = t.n_keys - g;
     first_leaf[i] = leaf;
     first_slot[i] = lb;
-    count[i] = want < rem ? want : rem;
+    if (end) {
+      int64_t g_end = t.n_keys;  // global rank of the first key > end
+      if (e != kMaxKey) {
+        const int32_t le = descend_leaf(t, f, e);
+        const int64_t *ke = t.leaf_rows + (int64_t)le * (li + 2 * lc) + li;
+        const int ce = __ldg(t.leaf_cnt + le);
+        int ub = 0;
+        while (ub < ce && __ldg(ke + ub) <= e) ub++;
+        g_end = __ldg(t.leaf_base + le) + ub;
+      }
+      count[i] = g_end > g ? g_end - g : 0;
+    } else {
+      const int64_t want = __ldg(len + i), rem = t.n_keys - g;
+      count[i] = want < rem ? want : rem;
+    }
   }
 }
 
@@ -273,10 +297,10 @@ size_t range_scratch_bytes(int64_t n) {
   return (size_t)align_up(n * 4, 256) * 2 + (size_t)align_up(n * 8, 256) + scan_scratch_bytes(n) + 256;
 }
 
-int range_locate(const hm_tree *t, const int64_t *start, const int32_t *len, int64_t n,
+int range_locate(const hm_tree *t, const int64_t *start, const int32_t *len, const int64_t *end, int64_t n,
                  int32_t *first_leaf, int32_t *first_slot, int64_t *count, cudaStream_t s) {
   range_locate_kernel<<<grid_for_items(n, 148u * 16), kThreads, 0, s>>>(
-      t->view(), t->cfg.fanout, t->cfg.leaf_cap, t->leaf_index, start, len, n, first_leaf,
+      t->view(), t->cfg.fanout, t->cfg.leaf_cap, t->leaf_index, start, len, end, n, first_leaf,
       first_slot, count);
   note_launch();
   return cuda_err(cudaGetLastError());

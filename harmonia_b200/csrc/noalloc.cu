@@ -1,13 +1,13 @@
 // hm_search_noalloc: the pre-sorted point search with its scratch memory in
 // a fixed device array instead of the tree's allocated scratch.
 //
-// Some callers cannot allocate device memory at the moment they search: code
-// running while a CUDA graph is being captured (cudaMalloc is not allowed
-// then), code inside a memory-budgeted serving loop that must not grow its
-// footprint, or a host runtime that reserves all device memory up front and
-// hands the library only its input and output buffers.  For them this entry
-// point takes its working space (the partitioned queries, their positions and
-// the histogram counters) from one file-scope __device__ array of fixed size,
+// Some callers cannot allocate device memory at the moment they search: a
+// host runtime that reserves all device memory up front and hands the library
+// only its input and output buffers, a serving loop held to a fixed
+// device-memory budget, or a latency-bound caller that cannot afford the
+// device-wide synchronisation cudaFree implies.  For them this entry point
+// takes its working space (the partitioned queries, their positions and the
+// histogram counters) from one file-scope __device__ array of fixed size,
 // created when the library is loaded, so a call never allocates.
 //
 // Rules of use:
@@ -15,8 +15,10 @@
 //  * Each GPU that loads the library holds the array (HM_NOALLOC_SCRATCH_BYTES)
 //    until the process exits.
 //  * The first call on a device looks the array's device address up
-//    (cudaGetSymbolAddress, with that device current) and caches it; make
-//    that first call before any stream capture.
+//    (cudaGetSymbolAddress, with that device current) and caches it; the
+//    search kernels' launch shapes are resolved then too.  Both caches serve
+//    the whole process, whichever thread calls next.  Make that first call
+//    before any stream capture.
 //  * All calls on a device share the one array, which keeps whatever the last
 //    call left in it: calls whose work overlaps on the GPU (different streams,
 //    or different trees searched concurrently) race and must be serialised by

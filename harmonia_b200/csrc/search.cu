@@ -29,6 +29,7 @@
 #include "async_copy.cuh"
 
 #include <cstdio>
+#include <mutex>
 
 namespace hm {
 
@@ -347,8 +348,12 @@ struct GridCache {
   int blocks_per_sm = 0;
 };
 
+// Resident CTAs per SM of a search kernel variant, looked up once per process
+// (any thread) and device: later launches make no occupancy query.
 int grid_for(const hm_tree *t, KernelFn fn, size_t smem, int *blocks) {
-  static thread_local GridCache cache[8];
+  static std::mutex mu;
+  static GridCache cache[64];
+  std::lock_guard<std::mutex> lk(mu);
   for (auto &c : cache)
     if (c.fn == fn && c.smem == smem && c.device == t->device) {
       *blocks = c.blocks_per_sm * t->num_sms;

@@ -295,7 +295,7 @@ int launch_ranges(hm_server *sv, Slot &sl) {
   cudaError_t e = cudaMemcpyAsync(ds, hs, n * 8, cudaMemcpyHostToDevice, sl.s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dl, hl, n * 4, cudaMemcpyHostToDevice, sl.s);
   if (e != cudaSuccess) return cuda_err(e);
-  rc = range_locate(t, ds, dl, n, fl, fs, cnt, sl.s);
+  rc = range_locate(t, ds, dl, nullptr, n, fl, fs, cnt, sl.s);
   if (rc) return rc;
   exclusive_scan_i64(cnt, off, n, scan, sl.s);
   rc = range_copy_out(t, fl, fs, off, n, ok, ov, sl.s);

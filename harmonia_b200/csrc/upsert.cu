@@ -490,8 +490,7 @@ size_t al(int64_t bytes) { return (size_t)align_up(bytes, 256); }
 // Bulk-loads n1 sorted (sign-flipped) keys and their values into a fresh arena
 // with the tree's parameters and swaps it in; the old arena is freed.
 int rebuild_from_sorted(hm_tree *t, const uint64_t *ck, const int64_t *cv, int64_t n1, cudaStream_t s) {
-  hm_tree nt = *t;  // new shape in a copy; arena swapped in at the end
-  nt.scratch = nullptr;
+  BuildTarget nt = t->target();  // new shape; the arena is swapped in at the end
   int rc = shape(n1, t->cfg, &nt.height, nt.lvl_start, &nt.n_inner, &nt.n_leaf);
   if (rc) return rc;
   size_t off_prefix = al(nt.n_inner * nt.inner_row * 8);
@@ -501,35 +500,34 @@ int rebuild_from_sorted(hm_tree *t, const uint64_t *ck, const int64_t *cv, int64
   size_t total = off_lbase + al(nt.n_leaf * 8);
   int64_t tn = std::max<int64_t>(std::max<int64_t>(n1, nt.n_leaf), 1);
   char *tmp = nullptr;
-  cudaError_t e = cudaMalloc(&nt.arena, total);
+  void *arena = nullptr;
+  cudaError_t e = cudaMalloc(&arena, total);
   if (e == cudaSuccess) e = cudaMalloc(&tmp, 2 * al(8 * tn));
   if (e != cudaSuccess) {
-    if (nt.arena) cudaFree(nt.arena);
+    if (arena) cudaFree(arena);
     if (tmp) cudaFree(tmp);
     return cuda_err(e);
   }
   int64_t *tmp_a = reinterpret_cast<int64_t *>(tmp);
   int64_t *tmp_b = reinterpret_cast<int64_t *>(tmp + al(8 * tn));
-  char *base = static_cast<char *>(nt.arena);
+  char *base = static_cast<char *>(arena);
   cudaMemsetAsync(base, 0, total, s);
-  nt.arena_bytes = total;
   nt.inner = reinterpret_cast<int64_t *>(base);
   nt.prefix = reinterpret_cast<int32_t *>(base + off_prefix);
   nt.leaf_rows = reinterpret_cast<int64_t *>(base + off_lrows);
   nt.leaf_cnt = reinterpret_cast<int32_t *>(base + off_lcnt);
   nt.leaf_base = reinterpret_cast<int64_t *>(base + off_lbase);
-  nt.n_keys = n1;
-  rc = build_from_sorted(&nt, ck, cv, n1, tmp_a, tmp_b, s);
+  rc = build_from_sorted(nt, ck, cv, n1, tmp_a, tmp_b, s);
   e = cudaStreamSynchronize(s);
   cudaFree(tmp);
   if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
   if (rc) {
-    cudaFree(nt.arena);
+    cudaFree(arena);
     return rc;
   }
   cudaFree(t->arena);
-  t->arena = nt.arena;
-  t->arena_bytes = nt.arena_bytes;
+  t->arena = arena;
+  t->arena_bytes = total;
   t->inner = nt.inner;
   t->prefix = nt.prefix;
   t->leaf_rows = nt.leaf_rows;
@@ -557,9 +555,10 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   const size_t mk4 = al(4 * (t->n_inner + 1));  // subtree marks, one per last-level node
   size_t need = 9 * s8 + 7 * s4 + lb8 + mk4 + al((int64_t)radix_scratch_bytes(n)) +
                 al((int64_t)scan_scratch_bytes(scan_n)) + 256;
-  int rc = ensure_scratch(t, need);
+  ScratchLease lease(t, s);
+  int rc = lease.acquire(need);
   if (rc) return rc;
-  char *p = static_cast<char *>(t->scratch);
+  char *p = static_cast<char *>(lease.ptr());
   auto take8 = [&](void) { char *r = p; p += s8; return r; };
   auto take4 = [&](void) { char *r = p; p += s4; return r; };
   uint64_t *uk = reinterpret_cast<uint64_t *>(take8());
@@ -722,9 +721,10 @@ int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed_
   const size_t lb8 = al(8 * (t->n_leaf + 1));
   size_t need = 6 * s8 + 2 * s4 + lb8 + al((int64_t)radix_scratch_bytes(n)) +
                 al((int64_t)scan_scratch_bytes(scan_n)) + 256;
-  int rc = ensure_scratch(t, need);
+  ScratchLease lease(t, s);
+  int rc = lease.acquire(need);
   if (rc) return rc;
-  char *p = static_cast<char *>(t->scratch);
+  char *p = static_cast<char *>(lease.ptr());
   auto take8 = [&](void) { char *r = p; p += s8; return r; };
   auto take4 = [&](void) { char *r = p; p += s4; return r; };
   uint64_t *uk = reinterpret_cast<uint64_t *>(take8());

@@ -15,7 +15,8 @@ defined by a seed and reproduced exactly on any machine:
 * Zipf(theta) queries over key rank (rank 0 = smallest key is hottest), drawn
   with the closed-form sampler of Gray et al., "Quickly generating
   billion-record synthetic databases" (SIGMOD'94).
-* range queries: start uniform, length uniform in [lo, hi].
+* range queries: start uniform, length uniform in [lo, hi]; inclusive ranges:
+  start uniform, end = start + about L keys' spacing.
 
 splitmix64 is the generator of Steele, Lea and Flood (OOPSLA'14).
 """
@@ -118,6 +119,22 @@ def gen_ranges(m: int, lo: int, hi: int, seed: int = 4):
     return start, length
 
 
+def gen_range_pairs(m: int, n_keys: int, lo: int, hi: int, seed: int = 4):
+    """m inclusive ranges (start, end) over a tree of about n_keys uniform
+    keys: start as gen_ranges, end = start + L * gap - 1 with L uniform in
+    [lo, hi] and gap = 2^63 / n_keys the mean key spacing, so a range holds
+    about L keys.  Every 64th range is empty (end = start - 1).  end stays
+    below Max_Key (the reference's descent asserts for that key)."""
+    start, length = gen_ranges(m, lo, hi, seed)
+    gap = np.uint64((2**63) // max(n_keys, 1))
+    with np.errstate(over="ignore"):
+        e = start.astype(np.uint64) + length.astype(np.uint64) * gap - np.uint64(1)
+    e = np.minimum(e, np.uint64(2**63 - 2)).astype(np.int64)
+    empty = (np.arange(m) % 64) == 63
+    e[empty] = start[empty] - 1
+    return start, e
+
+
 def _first_unique(a: np.ndarray) -> np.ndarray:
     """Distinct elements of a in order of first appearance."""
     _, idx = np.unique(a, return_index=True)
@@ -152,3 +169,62 @@ def gen_upserts(keys: np.ndarray, m: int, new_frac: float = 0.5, seed: int = 5):
     is_old = np.isin(bk, old)
     bv = np.where(is_old, bk - 1, values_for(bk))
     return bk.astype(np.int64), bv.astype(np.int64)
+
+
+def _unit(r: np.ndarray) -> np.ndarray:
+    """Uniform doubles in [0, 1) from uint64 draws (top 53 bits)."""
+    return (r >> np.uint64(11)).astype(np.float64) / float(1 << 53)
+
+
+def gen_uneven_batches(keys: np.ndarray, sorted_keys: np.ndarray, nb: int = 512, seed: int = 7,
+                       lo: int = 1024, hi: int = 4 << 20, pool_n: int = 1 << 24):
+    """The uneven multi-batch workload: nb batches with sizes log-uniform in
+    [lo, hi]; even batches draw from a pool of uniform point queries (90%
+    hits), odd ones from a pool of Zipf(0.99) queries over key rank; batch b is
+    a wrapped run of its pool starting at a seeded offset.  Returns (sizes,
+    queries): queries is one array holding the batches back to back."""
+    r = splitmix64(np.arange(nb, dtype=np.uint64) + np.uint64(seed) * np.uint64(1 << 40))
+    sizes = np.exp(np.log(lo) + _unit(r) * (np.log(hi) - np.log(lo))).astype(np.int64)
+    pools = (gen_point_queries(keys, pool_n, 0.9, seed + 1), gen_zipf_queries(sorted_keys, pool_n, 0.99, seed + 2))
+    out = np.empty(int(sizes.sum()), np.int64)
+    o = 0
+    for b in range(nb):
+        m = int(sizes[b])
+        start = int(r[b] % np.uint64(pool_n))
+        idx = (np.arange(m, dtype=np.int64) + start) % pool_n
+        out[o:o + m] = pools[b % 2][idx]
+        o += m
+    return sizes, out
+
+
+def gen_serving_stream(keys: np.ndarray, count: int, seed: int = 11, lo: int = 64, hi: int = 1 << 20):
+    """A seeded serving request stream over a tree holding ``keys``: sizes
+    log-uniform in [lo, hi]; 90% point searches (80% hits), 5% range requests
+    (size/64 ranges, length uniform in [1, 128]), 5% upserts (size/16 keys,
+    2..64: half new keys with value splitmix64(key)>>1, half existing keys with
+    value key-1, the reference's update rule).  Returns a list of
+    ("search", q) / ("range", start, length) / ("upsert", keys, values)."""
+    n = len(keys)
+    r = splitmix64(np.arange(3 * count, dtype=np.uint64) + np.uint64(seed) * np.uint64(1 << 40)).reshape(count, 3)
+    kind = _unit(r[:, 0])
+    sizes = np.exp(np.log(lo) + _unit(r[:, 1]) * (np.log(hi) - np.log(lo))).astype(np.int64)
+    fresh = gen_keys(1 << 20, seed + 100)
+    fresh = fresh[~np.isin(fresh, keys)]
+    at = 0
+    out = []
+    for i in range(count):
+        m = int(sizes[i])
+        sub = seed * 1_000_003 + i
+        if kind[i] < 0.90:
+            out.append(("search", gen_point_queries(keys, m, 0.8, sub)))
+        elif kind[i] < 0.95:
+            st, ln = gen_ranges(max(1, m // 64), 1, 128, sub)
+            out.append(("range", st, ln))
+        else:
+            k = max(2, min(m // 16, 64))
+            nk = fresh[at:at + k // 2]
+            at += k // 2
+            ek = keys[(splitmix64(np.arange(k - k // 2, dtype=np.uint64) + r[i, 2]) % np.uint64(n)).astype(np.int64)]
+            out.append(("upsert", np.concatenate([nk, ek]), np.concatenate([values_for(nk), ek - 1])))
+    return out
+

@@ -17,13 +17,14 @@ ERRORS = {
     -6: "HM_ECAPACITY", -7: "HM_ETIMEOUT", -8: "HM_ENODEVICE", -9: "HM_EBUSY",
     -10: "HM_ECANCELLED", -11: "HM_ETOOLARGE", -12: "HM_EIO",
 }
+HM_ECAPACITY = -6
 HM_UPSERT_SUPPLIED = 0
 HM_UPSERT_REF_KEY_MINUS_1 = 1
 
 # Every symbol include/harmonia.h declares.
 EXPORTS = (
     "hm_config_default", "hm_bulk_load", "hm_search", "hm_search_batches", "hm_range",
-    "hm_upsert_batch", "hm_export", "hm_tree_get_info", "hm_set_search_config",
+    "hm_range_between",    "hm_upsert_batch", "hm_export", "hm_tree_get_info", "hm_set_search_config",
     "hm_get_config", "hm_autotune", "hm_sync", "hm_free", "hm_strerror", "hm_launch_count",
     "hm_profile", "hm_profile_read", "hm_plan_create", "hm_plan_launch", "hm_plan_free",
     "hm_search_noalloc", "hm_server_config_default", "hm_server_start", "hm_server_submit",
@@ -95,6 +96,7 @@ def lib() -> ctypes.CDLL:
     L.hm_search.argtypes = [P, P, SZ, P, P]
     L.hm_search_batches.argtypes = [P, ctypes.POINTER(Batch), I, P]
     L.hm_range.argtypes = [P, P, P, SZ, P, P, P, SZ, ctypes.POINTER(SZ), P]
+    L.hm_range_between.argtypes = [P, P, P, SZ, P, P, P, SZ, ctypes.POINTER(SZ), P]
     L.hm_upsert_batch.argtypes = [P, P, P, SZ, I, P]
     L.hm_export.argtypes = [P, P, P, SZ, ctypes.POINTER(SZ)]
     L.hm_tree_get_info.argtypes = [P, ctypes.POINTER(TreeInfo)]

@@ -199,6 +199,36 @@ class BPlusTree:
         m = total.value
         return offsets, okeys[:m], ovals[:m]
 
+    def range_between(self, start, end, cap=None, stream=None):
+        """Inclusive ranges, as the reference's BPlusTree::range_search:
+        every record with start[i] <= key <= end[i].  Returns (offsets[n+1],
+        keys, values).  cap bounds the record count (default: counted by a
+        first call that returns HM_ECAPACITY with the total)."""
+        start = _as_i64(start)
+        end = _as_i64(end)
+        if len(start) != len(end):
+            raise ValueError("start and end differ in length")
+        n = len(start)
+        offsets = _empty_like(start, n + 1)
+        total = ctypes.c_size_t()
+
+        def call(c, ok, ov):
+            return lib().hm_range_between(self._h, _ptr(start) if n else None, _ptr(end) if n else None, n,
+                                          _ptr(offsets), _ptr(ok) if ok is not None else None,
+                                          _ptr(ov) if ov is not None else None, c, ctypes.byref(total),
+                                          _stream_ptr(stream))
+
+        if cap is None:
+            rc = call(0, None, None)
+            if rc not in (0, native.HM_ECAPACITY):
+                check(rc, "hm_range_between")
+            cap = total.value
+        okeys = _empty_like(start, max(cap, 1))
+        ovals = _empty_like(start, max(cap, 1))
+        check(call(cap, okeys, ovals), "hm_range_between")
+        m = total.value
+        return offsets, okeys[:m], ovals[:m]
+
     # ---- updates ----
     def delete(self, keys, stream=None) -> int:
         """One delete epoch: removes the stored keys among keys; returns how

@@ -18,8 +18,21 @@
  * (detected per call).  With device buffers a call only enqueues work on the
  * given stream and returns; with host buffers it copies in chunks through
  * pinned staging, overlapping copies with the search, and returns when the
- * results are in host memory.  Calls on one tree are serialised by the caller;
- * read-only calls (search, range) may run concurrently on different streams.
+ * results are in host memory.
+ *
+ * Concurrency.  Read-only calls on one tree (hm_search, hm_range,
+ * hm_search_batches, hm_export, hm_search_baseline) may be issued from any
+ * host threads on any streams, and their work may overlap on the device: each
+ * call leases a scratch block of its own from the tree's pool, ordered on the
+ * device after that block's previous use, and a block grows by a
+ * stream-ordered free and allocation, never by a device-wide synchronisation.
+ * Host-buffer searches of one tree take turns (they share the tree's copy
+ * streams and pinned staging).  Calls that change the tree or its settings
+ * (hm_upsert_batch, hm_delete_batch, hm_set_search_config, hm_autotune,
+ * hm_free) must not overlap any other call on the same tree, on the host or
+ * on the device.  Calls that need scratch return HM_EINVAL on a stream under
+ * graph capture; hm_plan_create captures searches with memory of its own.
+ * hm_search_noalloc has its own rule (one shared array per device).
  */
 #ifndef HARMONIA_H
 #define HARMONIA_H
@@ -153,6 +166,20 @@ int hm_range(hm_tree *t, const int64_t *start, const int32_t *len, size_t n,
              int64_t *offsets, int64_t *okeys, int64_t *ovals, size_t cap,
              size_t *total, hm_stream s);
 
+/* Inclusive range scan: for query i every record with start[i] <= key <=
+ * end[i], in key order (none when end[i] < start[i]; end[i] = INT64_MAX runs
+ * to the end of the key space), compacted as hm_range: offsets has n+1
+ * entries, *total receives offsets[n], HM_ECAPACITY (with *total set) when
+ * cap is too small.  start and end may be host or device memory, as may the
+ * outputs.  Pairs read by hm_read_ranges from a reference range file can be
+ * passed as they are.
+ * Replaces: BPlusTree::range_search(start_key, end_key, &records)
+ * (open-harmonia/src/bpt.cpp:695-769) and the CFB find_range
+ * (open-harmonia/regular_bpt/regular_bpt.cpp:320-340). */
+int hm_range_between(hm_tree *t, const int64_t *start, const int64_t *end, size_t n,
+                     int64_t *offsets, int64_t *okeys, int64_t *ovals, size_t cap,
+                     size_t *total, hm_stream s);
+
 #define HM_UPSERT_SUPPLIED 0        /* an existing key takes the supplied value */
 #define HM_UPSERT_REF_KEY_MINUS_1 1 /* an existing key takes key-1, as the reference does */
 
@@ -251,20 +278,24 @@ int hm_server_stop(hm_server *sv);
 /* Stops if needed and frees the server and every uncollected request. */
 int hm_server_free(hm_server *sv);
 
-/* Point search that allocates nothing, for callers that cannot allocate
- * device memory when they search: code running while a CUDA graph is being
- * captured, a serving loop held to a fixed memory budget, or a host runtime
- * that owns all device memory and hands the library only its buffers.  It
- * runs the same pre-sort (8 bits) and search as hm_search, with its working
- * space in one fixed array the library keeps in device memory
+/* Point search that allocates nothing.  Some callers cannot allocate device
+ * memory at the moment they search: a host runtime that reserves all device
+ * memory up front and hands the library only its input and output buffers (a
+ * database's GPU buffer manager, a framework's caching allocator), a serving
+ * loop held to a fixed device-memory budget, or a latency-bound caller that
+ * cannot afford the device-wide synchronisation cudaFree implies.  This entry
+ * point runs the same pre-sort (8 bits) and search as hm_search, with its
+ * working space in one fixed array the library keeps in device memory
  * (HM_NOALLOC_SCRATCH_BYTES on every GPU that loads the library, held until
  * the process exits).  q and out must be device memory, n at most
  * HM_NOALLOC_MAX_QUERIES (HM_ETOOLARGE otherwise, HM_EINVAL for host
- * buffers).  Only enqueues on s.  The first call on a device looks the
- * array's address up; make it before any stream capture.  All calls on a
- * device share the array: calls that overlap on the GPU race, so serialise
- * them.  No counterpart in the reference, whose drivers cudaMalloc their
- * buffers per experiment (open-harmonia/src/full-multi-prefix-sort-8thread.cu:409-433). */
+ * buffers).  Only enqueues on s.  The first call on each device looks the
+ * array's device address up and resolves the kernels' launch shapes (both
+ * kept for the whole process, whichever thread calls next); make that first
+ * call before any stream capture.  All calls on a device share the array,
+ * which keeps whatever the last call left in it: calls that overlap on the
+ * GPU (other streams, threads or trees) race, so serialise them.  It has no
+ * counterpart in the reference. */
 #define HM_NOALLOC_MAX_QUERIES (1 << 20)
 #define HM_NOALLOC_SCRATCH_BYTES (14u << 20)
 int hm_search_noalloc(hm_tree *t, const int64_t *q, size_t n, int64_t *out, hm_stream s);

@@ -231,6 +231,41 @@ int64_t hmo_range(const hmo_tree *t, const int64_t *start, const int32_t *len,
   return total;
 }
 
+/* Inclusive ranges, as BPlusTree::range_search (open-harmonia/src/bpt.cpp:695-769)
+ * returns them: every record with start <= key <= end in ascending key order,
+ * nothing when start > end.  The reference finds the start key's lower bound
+ * (findKeyLowerBound, bpt.h:289-297) and the end key's upper bound
+ * (findKeyUpperBound, bpt.h:298-306) and copies everything between them leaf
+ * after leaf; here the walk from the lower bound stops at the first key > end. */
+int64_t hmo_range_between(const hmo_tree *t, const int64_t *start, const int64_t *end,
+                          int64_t n, int64_t *offsets, int64_t *okeys, int64_t *ovals,
+                          int64_t cap) {
+  int64_t total = 0;
+  for (int64_t i = 0; i < n; i++) {
+    offsets[i] = total;
+    if (start[i] > end[i] || start[i] == HMO_MAX_KEY || t->n_keys == 0) continue;
+    int64_t leaf = descend(t, start[i]);
+    int slot = 0; /* lower bound: first key >= start */
+    while (slot < t->leaf_cnt[leaf] && t->leaf_rows[leaf * t->leaf_row + t->leaf_index + slot] < start[i]) slot++;
+    while (leaf < t->n_leaf) {
+      if (slot >= t->leaf_cnt[leaf]) {
+        leaf++;
+        slot = 0;
+        continue;
+      }
+      const int64_t *r = t->leaf_rows + leaf * t->leaf_row + t->leaf_index;
+      if (r[slot] > end[i]) break;
+      if (total >= cap) return -1;
+      okeys[total] = r[slot];
+      ovals[total] = r[t->p.leaf_cap + slot];
+      total++;
+      slot++;
+    }
+  }
+  offsets[n] = total;
+  return total;
+}
+
 int64_t hmo_export(const hmo_tree *t, int64_t *keys, int64_t *vals, int64_t cap) {
   if (cap < t->n_keys) return -1;
   int64_t o = 0;

@@ -70,6 +70,12 @@ int64_t hmo_range(const hmo_tree *t, const int64_t *start, const int32_t *len,
                   int64_t n, int64_t *offsets, int64_t *okeys, int64_t *ovals,
                   int64_t cap);
 
+/* Inclusive ranges: every record with start[i] <= key <= end[i]; returns
+ * total records, or -1 if cap is too small.  offsets has n+1 entries. */
+int64_t hmo_range_between(const hmo_tree *t, const int64_t *start, const int64_t *end,
+                          int64_t n, int64_t *offsets, int64_t *okeys, int64_t *ovals,
+                          int64_t cap);
+
 /* Sorted contents; returns count, or -1 if cap is too small. */
 int64_t hmo_export(const hmo_tree *t, int64_t *keys, int64_t *vals, int64_t cap);
 

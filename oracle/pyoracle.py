@@ -68,6 +68,8 @@ def _port_lib():
         lib.hmo_search.argtypes = [ctypes.POINTER(_Tree), _P, _I64, _P]
         lib.hmo_range.argtypes = [ctypes.POINTER(_Tree), _P, _P, _I64, _P, _P, _P, _I64]
         lib.hmo_range.restype = _I64
+        lib.hmo_range_between.argtypes = [ctypes.POINTER(_Tree), _P, _P, _I64, _P, _P, _P, _I64]
+        lib.hmo_range_between.restype = _I64
         lib.hmo_export.argtypes = [ctypes.POINTER(_Tree), _P, _P, _I64]
         lib.hmo_export.restype = _I64
         lib.hmo_upsert.argtypes = [_P, _P, _I64, _P, _P, _I64, ctypes.c_int, _P, _P, _I64]
@@ -155,6 +157,22 @@ class PortTree:
         tot = _port_lib().hmo_range(ctypes.byref(self.t), _ptr(start), _ptr(length), n, _ptr(off), _ptr(ok), _ptr(ov), cap)
         return off, ok[:tot], ov[:tot]
 
+    def range_between(self, start, end):
+        """Inclusive ranges: every record with start[i] <= key <= end[i]."""
+        start = np.ascontiguousarray(start, dtype=np.int64)
+        end = np.ascontiguousarray(end, dtype=np.int64)
+        n = len(start)
+        off = np.empty(n + 1, np.int64)
+        cap = max(4 * n, 1 << 12)
+        while True:
+            ok = np.empty(cap, np.int64)
+            ov = np.empty(cap, np.int64)
+            tot = _port_lib().hmo_range_between(ctypes.byref(self.t), _ptr(start), _ptr(end), n, _ptr(off),
+                                                _ptr(ok), _ptr(ov), cap)
+            if tot >= 0:
+                return off, ok[:tot], ov[:tot]
+            cap *= 4
+
     def export(self):
         n = self.t.n_keys
         k = np.empty(max(n, 1), np.int64)
@@ -205,6 +223,8 @@ def _ref_lib():
         lib.hmref_search.argtypes = [_P, _P, _L, _P, ctypes.c_int]
         lib.hmref_range.argtypes = [_P, _P, _P, _L, _P, _P, _P, _L]
         lib.hmref_range.restype = _L
+        lib.hmref_range_between.argtypes = [_P, _P, _P, _L, _P, _P, _P, _L, ctypes.c_int]
+        lib.hmref_range_between.restype = _L
         lib.hmref_upsert.argtypes = [_P, _P, _P, _L, _L, _L]
         lib.hmref_upsert.restype = ctypes.c_int
         lib.hmref_export.argtypes = [_P, _P, _P, _L]
@@ -243,6 +263,25 @@ class RefTree:
         ov = np.empty(max(cap, 1), np.int64)
         tot = _ref_lib().hmref_range(self.h, _ptr(start), _ptr(length), n, _ptr(off), _ptr(ok), _ptr(ov), cap)
         return off, ok[:tot], ov[:tot]
+
+    def range_between(self, start, end, walk: bool = False):
+        """Inclusive ranges by BPlusTree::range_search: every record with
+        start[i] <= key <= end[i] (offsets, keys, values, compacted).  After
+        an update, or with walk=True, the same walk over the update-aware
+        descent (ref_driver.cpp range_between_walk)."""
+        start = np.ascontiguousarray(start, dtype=np.int64)
+        end = np.ascontiguousarray(end, dtype=np.int64)
+        n = len(start)
+        off = np.empty(n + 1, np.int64)
+        cap = max(4 * n, 1 << 12)
+        while True:
+            ok = np.empty(cap, np.int64)
+            ov = np.empty(cap, np.int64)
+            tot = _ref_lib().hmref_range_between(self.h, _ptr(start), _ptr(end), n, _ptr(off), _ptr(ok),
+                                                 _ptr(ov), cap, 1 if walk else 0)
+            if tot >= 0:
+                return off, ok[:tot], ov[:tot]
+            cap *= 4
 
     def upsert(self, keys, vals, syn_batch: int = 0, rebuild_batch: int = 0) -> None:
         keys = np.ascontiguousarray(keys, dtype=np.int64)

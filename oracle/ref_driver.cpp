@@ -136,6 +136,96 @@ long hmref_range(void *hp, const long long *start, const int *len, long n,
   return total;
 }
 
+}  // extern "C"
+
+namespace {
+
+// BPlusTree::range_search (bpt.cpp:695-769) from its descent on: the walk
+// over big leaves and record lists between the start key's lower bound and
+// the end key's upper bound, appending to v, with the leaves located by the
+// Newupdate descent (leaf_for), which stays valid after updates.  The walk
+// keeps the reference's steps, including the step back to the previous big
+// leaf when the end key's record list holds nothing <= end.
+void range_between_walk(BPlusTree *t, key_t start_key, key_t end_key, std::vector<Record> *v) {
+  if (start_key > end_key) return;
+  int relist_idx_start = 0, relist_idx_end = 0;
+  BLeaf_node *blfnode_start =
+      leaf_for(t, t->search_last_level_inner_node_PPItree_Newupdate(start_key), start_key, relist_idx_start);
+  BLeaf_node *blfnode_end =
+      leaf_for(t, t->search_last_level_inner_node_PPItree_Newupdate(end_key), end_key, relist_idx_end);
+  int idx_start = blfnode_start->findKeyLowerBound(relist_idx_start, start_key);
+  int idx_end = blfnode_end->findKeyUpperBound(relist_idx_end, end_key);
+  if (idx_start == -1) {
+    idx_start = 0;
+    relist_idx_start++;
+    if (relist_idx_start >= blfnode_start->used_relist_slot_num) {
+      if (blfnode_start == blfnode_end) return;
+      blfnode_start = blfnode_start->next;
+      relist_idx_start = 0;
+    }
+  }
+  if (idx_end == -1) {
+    relist_idx_end--;
+    if (relist_idx_end < 0) {
+      if (blfnode_start == blfnode_end) return;
+      BLeaf_node *temp = blfnode_start, *temp1 = blfnode_start;
+      while (temp != blfnode_end) {
+        temp1 = temp;
+        temp = temp->next;
+      }
+      blfnode_end = temp1;
+      relist_idx_end = -1;
+    }
+  }
+  if (blfnode_start == blfnode_end) {
+    blfnode_start->getKeyValuesRange(relist_idx_start, relist_idx_end, idx_start, idx_end, v);
+    return;
+  }
+  blfnode_start->getKeyValuesRange(relist_idx_start, -1, idx_start, -1, v);
+  for (blfnode_start = blfnode_start->next; blfnode_start != blfnode_end; blfnode_start = blfnode_start->next) {
+    if (blfnode_start == nullptr) return;
+    blfnode_start->getKeyValuesRange(0, -1, 0, -1, v);
+  }
+  blfnode_end->getKeyValuesRange(0, relist_idx_end, 0, idx_end, v);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Inclusive ranges: for query i every record with start[i] <= key <= end[i]
+// in ascending key order (nothing when start > end).  Before any update this
+// calls BPlusTree::range_search itself (bpt.cpp:695-769); after an update,
+// whose new nodes its pointer descent does not follow (it crashes there),
+// the same walk with the Newupdate descent (range_between_walk).  walk != 0
+// forces the walk (to check it against range_search).  end must not be
+// Max_Key: the reference's descent asserts for that key on a PPI tree
+// (mempool.h:51).  offsets has n+1 entries.  Returns the total number of
+// records, or -1 if cap is too small.
+long hmref_range_between(void *hp, const long long *start, const long long *end, long n,
+                         long long *offsets, long long *okeys, long long *ovals, long cap, int walk) {
+  RefTree *h = static_cast<RefTree *>(hp);
+  BPlusTree *t = h->ppi;
+  long total = 0;
+  std::vector<Record> v;
+  for (long i = 0; i < n; i++) {
+    offsets[i] = total;
+    v.clear();
+    if (h->updated || walk)
+      range_between_walk(t, start[i], end[i], &v);
+    else
+      t->range_search(start[i], end[i], &v);
+    if (total + (long)v.size() > cap) return -1;
+    for (const Record &r : v) {
+      okeys[total] = r.r_key;
+      ovals[total] = r.val;
+      total++;
+    }
+  }
+  offsets[n] = total;
+  return total;
+}
+
 // One update batch through the reference's parallel update.  syn_batch and
 // rebuild_batch are the reference's two batch sizes; the reference reads past
 // the input unless n is a multiple of syn_batch, so other values are clamped

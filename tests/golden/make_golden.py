@@ -4,7 +4,7 @@ Run in a container that has the reference sources (it builds
 oracle/_ref/libhmref.so from them with `make -C oracle ref`):
 
     python tests/golden/make_golden.py          # 2^20-key cases + small arrays
-    python tests/golden/make_golden.py --big    # adds the 2^26-key cases (~10 min)
+    python tests/golden/make_golden.py --big    # adds the 2^26- and 2^25-key cases (~30 min)
 
 Every input comes from harmonia_b200.datagen with the seeds recorded in
 golden.json, so a test regenerates the inputs bit for bit and compares the
@@ -51,6 +51,47 @@ def range_case(ref, m, lo, hi, seed):
     return {"m": m, "lo": lo, "hi": hi, "seed": seed, "digest": digest(off, k, v), "records": int(len(k))}
 
 
+def range_between_case(ref, m, n_keys, lo, hi, seed):
+    st, en = dg.gen_range_pairs(m, n_keys, lo, hi, seed)
+    off, k, v = ref.range_between(st, en)
+    return {"m": m, "n_keys": n_keys, "lo": lo, "hi": hi, "seed": seed, "digest": digest(off, k, v),
+            "records": int(len(k))}
+
+
+def batches_case(ref, keys, sk, nb, seed):
+    """C4: per-batch digests of the uneven batch set (datagen.gen_uneven_batches)."""
+    sizes, q = dg.gen_uneven_batches(keys, sk, nb, seed)
+    res = ref.search(q)
+    ends = np.concatenate([[0], np.cumsum(sizes)])
+    return {"nb": nb, "seed": seed, "queries": int(len(q)), "digest": digest(res), "hits": int((res >= 0).sum()),
+            "batch_digests": [digest(res[ends[b]:ends[b + 1]]) for b in range(nb)]}
+
+
+def serving_replay_case(n, key_seed, count, seed):
+    """C5: the seeded serving stream (datagen.gen_serving_stream) replayed on
+    the reference in submission order: reads answered against the tree as
+    the upserts before them left it, upserts applied by the reference's
+    batched update."""
+    keys = dg.gen_keys(n, key_seed)
+    t0 = time.time()
+    ref = po.RefTree(keys, dg.values_for(keys))
+    build_s = time.time() - t0
+    stream = dg.gen_serving_stream(keys, count, seed)
+    reads = []
+    for req in stream:
+        if req[0] == "search":
+            reads.append(digest(ref.search(req[1])))
+        elif req[0] == "range":
+            off, k, v = ref.range(req[1], req[2])
+            reads.append(digest(off, k, v))
+        else:
+            ref.upsert(req[1], req[2])
+    ek, ev = ref.export()
+    return {"n": n, "key_seed": key_seed, "count": count, "seed": seed, "read_digests": reads,
+            "kinds": "".join(r[0][0] for r in stream), "export_digest": digest(ek, ev), "n_after": int(len(ek)),
+            "ref_build_s": round(build_s, 1)}
+
+
 def upsert_case(ref, keys, m, new_frac, seed):
     bk, bv = dg.gen_upserts(keys, m, new_frac, seed)
     ref.upsert(bk, bv)
@@ -77,7 +118,10 @@ def main():
     q = dg.gen_zipf_queries(np.sort(keys), 1 << 20, 0.99, 3)
     gold["c1_zipf"] = {"m": 1 << 20, "theta": 0.99, "q_seed": 3, "digest": digest(ref.search(q))}
     gold["c1_range"] = range_case(ref, 1 << 16, 1, 256, 4)
+    gold["c1_range_between"] = range_between_case(ref, 1 << 16, 1 << 20, 1, 256, 14)
     gold["c1_upsert"] = upsert_case(ref, keys, 1 << 14, 0.5, 5)
+    # inclusive ranges again after the epoch (the reference walk over the updated tree)
+    gold["c1_range_between_after"] = range_between_case(ref, 1 << 16, 1 << 20, 1, 256, 14)
     # a second epoch on the updated tree
     ek, _ = ref.export()
     gold["c1_upsert2"] = upsert_case(ref, ek, 1 << 14, 0.5, 6)
@@ -107,6 +151,20 @@ def main():
         q = dg.gen_zipf_queries(np.sort(keys), 1 << 24, 0.99, 3)
         gold["c3_zipf"] = {"m": 1 << 24, "theta": 0.99, "q_seed": 3, "digest": digest(ref.search(q))}
         gold["c3_range"] = range_case(ref, 1 << 20, 1, 256, 4)
+        gold["c3_range_between"] = range_between_case(ref, 1 << 20, 1 << 26, 1, 256, 15)
+        gold["c4_batches"] = batches_case(ref, keys, np.sort(keys), 512, 7)
+        # one update epoch at the paper's batch size: 4096K keys, 5% new
+        bk, bv = dg.gen_upserts(keys, 4 << 20, 0.05, 21)
+        t0 = time.time()
+        ref.upsert(bk, bv)
+        up_s = time.time() - t0
+        ek, ev = ref.export()
+        q = dg.gen_point_queries(keys, 1 << 24, 0.9, 2)
+        gold["c2_upsert_4096k"] = {"m": 4 << 20, "new_frac": 0.05, "seed": 21, "export_digest": digest(ek, ev),
+                                   "n_after": int(len(ek)), "search_batch_digest": digest(ref.search(bk)),
+                                   "search_c2_digest": digest(ref.search(q)), "ref_upsert_s": round(up_s, 1)}
+        del ref, ek, ev
+        gold["c5_serving_replay"] = serving_replay_case(1 << 25, 11, 400, 11)
     with open(path, "w") as f:
         json.dump(gold, f, indent=1, sort_keys=True)
     print(json.dumps(gold, indent=1, sort_keys=True))

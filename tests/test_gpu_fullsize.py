@@ -1,7 +1,10 @@
 """GPU parity at the benchmark's full sizes, pinned by the reference's own
 digests: a 2^26-key tree at fanout 64 and 128, 2^24 point queries (90% hits,
-unsorted and pre-sorted), 2^24 Zipf(0.99) queries and 2^20 ranges of 1..256
-records (golden.json: c2_point, c3_zipf, c3_range)."""
+unsorted and pre-sorted), 2^24 Zipf(0.99) queries, 2^20 ranges of 1..256
+records and 2^20 inclusive ranges of about as many keys, 512 uneven batches
+(1K..4M queries, uniform and Zipf) searched as one set, and one upsert epoch
+of 4096K keys (5% new) (golden.json: c2_point, c3_zipf, c3_range,
+c3_range_between, c4_batches, c2_upsert_4096k)."""
 import numpy as np
 import pytest
 
@@ -52,3 +55,77 @@ def test_c3_zipf_and_range_full_size(big):
         off, k, v = t.range_search(torch.from_numpy(st).cuda(), torch.from_numpy(ln).cuda())
         assert len(k) == g["records"]
         assert digest(off.cpu().numpy(), k.cpu().numpy(), v.cpu().numpy()) == g["digest"]
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_c3_range_between_full_size(big):
+    keys, sk = big
+    g = GOLD["c3_range_between"]
+    st, en = dg.gen_range_pairs(g["m"], g["n_keys"], g["lo"], g["hi"], g["seed"])
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys))) as t:
+        off, k, v = t.range_between(cuda(st), cuda(en))
+        assert len(k) == g["records"]
+        assert digest(off.cpu().numpy(), k.cpu().numpy(), v.cpu().numpy()) == g["digest"]
+
+
+def test_c4_uneven_batches_full_size(big):
+    """The 512-batch set through a captured plan (two replays, the second
+    after the outputs were overwritten) and through hm_search_batches; every
+    batch's results against the reference's digest of that batch."""
+    keys, sk = big
+    g = GOLD["c4_batches"]
+    sizes, q = dg.gen_uneven_batches(keys, sk, g["nb"], g["seed"])
+    assert len(q) == g["queries"]
+    ends = np.concatenate([[0], np.cumsum(sizes)])
+    dq = cuda(q)
+    out = torch.full_like(dq, -7)
+    batches = [(dq[ends[b]:ends[b + 1]], out[ends[b]:ends[b + 1]]) for b in range(g["nb"])]
+
+    def check(what):
+        res = out.cpu().numpy()
+        bad = [b for b in range(g["nb"]) if digest(res[ends[b]:ends[b + 1]]) != g["batch_digests"][b]]
+        assert not bad, f"{what}: batches {bad[:8]} differ"
+        assert digest(res) == g["digest"]
+
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys))) as t:
+        with t.plan(batches) as p:
+            for rep in range(2):
+                out.fill_(-7)
+                p.launch()
+                torch.cuda.synchronize()
+                check(f"plan replay {rep}")
+        out.fill_(-7)
+        t.search_batches(batches)
+        torch.cuda.synchronize()
+        check("hm_search_batches")
+
+
+@pytest.fixture(scope="module")
+def upsert_4096k(big):
+    keys, sk = big
+    g = GOLD["c2_upsert_4096k"]
+    bk, bv = dg.gen_upserts(keys, g["m"], g["new_frac"], g["seed"])
+    return bk, bv
+
+
+@pytest.mark.parametrize("leaf_fill,ref_rule", [(16, False), (12, True)])
+def test_c2_upsert_epoch_4096k_full_size(big, upsert_4096k, leaf_fill, ref_rule):
+    """One epoch at the paper's batch size (4096K keys, 5% new) on the 2^26-key
+    tree: with full leaves every touched leaf overflows (subtree rebalance or
+    rebuild); with 12 of 16 slots filled most new keys merge in place.  The
+    contents, the batch's own keys and the C2 query batch afterwards against
+    the reference's insert_parallel_Newupdate_batch."""
+    keys, sk = big
+    bk, bv = upsert_4096k
+    g = GOLD["c2_upsert_4096k"]
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), leaf_fill=leaf_fill) as t:
+        t.upsert(cuda(bk), cuda(bv), ref_rule=ref_rule)
+        ek, ev = t.export()
+        assert len(ek) == g["n_after"] and digest(ek, ev) == g["export_digest"]
+        assert digest(t.search(cuda(bk)).cpu().numpy()) == g["search_batch_digest"]
+        gq = GOLD["c2_point"]
+        q = dg.gen_point_queries(keys, gq["m"], gq["hit"], gq["q_seed"])
+        assert digest(t.search(cuda(q)).cpu().numpy()) == g["search_c2_digest"]

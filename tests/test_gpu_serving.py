@@ -156,3 +156,40 @@ def test_stop_cancels_queued_and_wait_times_out():
         with pytest.raises(HarmoniaError) as e:
             srv.search(keys[:10])
         assert e.value.code == -10
+
+
+def test_c5_serving_replay_matches_reference():
+    """The seeded serving stream on a 2^25-key tree (400 requests: point
+    searches, ranges and upsert epochs, sizes 64..2^20) submitted back to back
+    to a server with three launch slots: every read's result and the final
+    contents against the reference replaying the same stream in submission
+    order (golden.json c5_serving_replay)."""
+    from tests.helpers import digest, load_golden
+    g = load_golden()["c5_serving_replay"]
+    keys = dg.gen_keys(g["n"], g["key_seed"])
+    stream = dg.gen_serving_stream(keys, g["count"], g["seed"])
+    assert "".join(r[0][0] for r in stream) == g["kinds"]
+    tree = BPlusTree.bulk_load(torch.from_numpy(keys).cuda(), torch.from_numpy(dg.values_for(keys)).cuda(),
+                               leaf_fill=12)
+    with tree, Server(tree, streams=3, max_launch_queries=1 << 22, device_budget_bytes=2 << 30) as srv:
+        tickets = []
+        for req in stream:
+            if req[0] == "search":
+                tickets.append(srv.search(req[1]))
+            elif req[0] == "range":
+                tickets.append(srv.range(req[1], req[2]))
+            else:
+                tickets.append(srv.upsert(req[1], req[2]))
+        reads = []
+        for req, tk in zip(stream, tickets):
+            r = tk.wait()
+            if req[0] == "search":
+                reads.append(digest(r))
+            elif req[0] == "range":
+                reads.append(digest(*r))
+        bad = [i for i, (a, b) in enumerate(zip(reads, g["read_digests"])) if a != b]
+        assert len(reads) == len(g["read_digests"]) and not bad, f"reads {bad[:8]} differ"
+        st = srv.stats()
+        assert st["failed"] == 0 and st["completed"] == g["count"]
+        ek, ev = tree.export()
+        assert len(ek) == g["n_after"] and digest(ek, ev) == g["export_digest"]

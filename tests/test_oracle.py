@@ -145,3 +145,56 @@ def test_port_matches_reference_directly(n, fanout, leaf_cap):
     st[:2] = [sk[0], sk[-1]]
     a, b = ref.range(st, ln), t.range(st, ln)
     assert all((x == y).all() for x, y in zip(a, b))
+
+
+def test_port_matches_c1_range_between_digests(c1):
+    """Inclusive ranges (BPlusTree::range_search) before and after the first
+    C1 upsert epoch, on two layouts of the restatement."""
+    keys, sk, sv = c1
+    g = GOLD["c1_range_between"]
+    st, en = dg.gen_range_pairs(g["m"], g["n_keys"], g["lo"], g["hi"], g["seed"])
+    for fanout, leaf_cap in [(64, 16), (128, 64)]:
+        off, k, v = po.PortTree(sk, sv, fanout=fanout, leaf_cap=leaf_cap).range_between(st, en)
+        assert digest(off, k, v) == g["digest"] and len(k) == g["records"]
+    gu, ga = GOLD["c1_upsert"], GOLD["c1_range_between_after"]
+    bk, bv = dg.gen_upserts(keys, gu["m"], gu["new_frac"], gu["seed"])
+    ek, ev = po.upsert_set(sk, sv, bk, bv)
+    off, k, v = po.PortTree(ek, ev).range_between(st, en)
+    assert digest(off, k, v) == ga["digest"] and len(k) == ga["records"]
+
+
+def test_port_range_between_edges():
+    sk = np.arange(10, 1000, 10, dtype=np.int64)  # 10, 20, ..., 990
+    t = po.PortTree(sk, sk * 3, leaf_cap=16)
+    st = np.array([10, 15, 990, 995, -5, 500, 500, 0, 200], np.int64)
+    en = np.array([10, 25, 990, 2000, 5, 499, 500, po.MAX_KEY, 100], np.int64)
+    off, k, v = t.range_between(st, en)
+    want = [[10], [20], [990], [], [], [], [500], list(range(10, 1000, 10)), []]
+    assert np.diff(off).tolist() == [len(w) for w in want]
+    assert k.tolist() == sum(want, []) and (v == k * 3).all()
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference library not built in this checkout")
+@pytest.mark.parametrize("n", [5, 100, 5000, 1 << 16])
+def test_range_between_port_and_reference_walk_match_reference(n):
+    """The reference's own range_search, its walk over the update-aware
+    descent (used after updates), and the restatement agree; after an upsert
+    epoch the walk and the restatement on the upserted contents agree."""
+    keys = dg.gen_keys(n, seed=300 + n)
+    vals = dg.values_for(keys)
+    ref = po.RefTree(keys, vals)
+    sk = np.sort(keys)
+    st, en = dg.gen_range_pairs(3000, n, 1, 40, seed=n)
+    st[:4] = [sk[0], sk[-1], sk[n // 2], sk[0] - 1]
+    en[:4] = [sk[0], sk[-1] + 1, sk[n // 2] - 1, sk[min(3, n - 1)]]
+    a = ref.range_between(st, en)
+    b = ref.range_between(st, en, walk=True)
+    c = po.PortTree(sk, dg.values_for(sk)).range_between(st, en)
+    assert all((x == y).all() for x, y in zip(a, b))
+    assert all((x == y).all() for x, y in zip(a, c))
+    bk, bv = dg.gen_upserts(keys, max(2, n // 4), 0.5, seed=n + 1)
+    ref.upsert(bk, bv)
+    ek, ev = po.upsert_set(sk, dg.values_for(sk), bk, bv)
+    a = ref.range_between(st, en)
+    c = po.PortTree(ek, ev).range_between(st, en)
+    assert all((x == y).all() for x, y in zip(a, c))

@@ -1,9 +1,10 @@
 """The allocation-free search entry point, hm_search_noalloc.
 
-Some callers cannot allocate device memory when they search (a CUDA graph
-being captured, a serving loop held to a fixed budget, a host runtime that owns
-all device memory).  hm_search_noalloc serves them from a fixed array the
-library keeps in device memory.  This test calls it through the C ABI and
+Some callers cannot allocate device memory when they search: a host runtime
+that owns all device memory and hands the library only its buffers, a serving
+loop held to a fixed budget, or a caller that cannot afford the device-wide
+synchronisation cudaFree implies.  hm_search_noalloc serves them from a fixed
+array the library keeps in device memory.  This test calls it through the C ABI and
 checks it against the allocating entry point, hm_search, on two calls in a
 row (the second with other queries and another size, so whatever the first
 call left in the shared array must not matter).  Results are integers:
