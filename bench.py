@@ -59,6 +59,12 @@ def parse():
     return ap.parse_args()
 
 
+def workload_name(args) -> str:
+    """The workload both arms run, in words (the same string in both lines)."""
+    return (f"point search, 2^{args.keys_log2} keys (uniform 63-bit, value = splitmix64(key)>>1), fanout "
+            f"{args.fanout}, one 2^{args.queries_log2}-query batch, {int(args.hit * 100)}% hits")
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -137,6 +143,11 @@ def dist_init():
 
 
 def run_reference(args, ws, rank):
+    """The reference's own CPU tree (oracle/_ref/libhmref.so, built from
+    open-harmonia/src) on the same keys and the whole query batch per step:
+    OpenMP over BPlusTree::search on all host threads, the loop of
+    search_cpu_test (open-harmonia/src/main.cpp:772-812).  value = queries
+    per step over the median step time."""
     if rank != 0:
         return 0
     from harmonia_b200 import datagen as dg
@@ -151,8 +162,8 @@ def run_reference(args, ws, rank):
     t0 = time.time()
     ref = po.RefTree(keys, vals)
     build_s = time.time() - t0
-    m = min(1 << args.queries_log2, 1 << args.cpu_sample_log2)
-    q = dg.gen_point_queries(keys, 1 << args.queries_log2, args.hit, 2)[:m]
+    m = 1 << args.queries_log2
+    q = dg.gen_point_queries(keys, m, args.hit, 2)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         ref.search(q, threads)
@@ -161,23 +172,123 @@ def run_reference(args, ws, rank):
         a = time.perf_counter()
         ref.search(q, threads)
         times.append(time.perf_counter() - a)
-    sec = sum(times) / len(times)
+    sec = statistics.median(times)
     v = m / sec / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded splitmix64 keys/queries)",
-        "config": {"workload": f"point search, 2^{args.keys_log2}-key tree, fanout {args.fanout} (reference "
-                               f"HB-style PPI tree, BPT_ORDER 64), 2^{args.queries_log2}-query batch, "
-                               f"{int(args.hit * 100)}% hits", "queries_per_step": m},
+        "config": {"workload": workload_name(args), "queries_per_step": m, "statistic": "median of the steps",
+                   "layout": "the reference's PPI tree (BPT_ORDER 64 inner nodes, 64-list big leaves)"},
         "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{m} of the batch's queries per step, OpenMP BPlusTree::search over "
-                                   f"{threads} threads; tree build {build_s:.0f} s excluded"},
+                         "sample": f"the whole {m}-query batch per step, OpenMP BPlusTree::search over "
+                                   f"{threads} threads, median of {args.steps} steps; tree build {build_s:.0f} s "
+                                   "excluded"},
         "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
+    """Spawned helper process (no CUDA): builds one of the reference's CPU
+    trees of the bench workload while the GPU legs run (the build is serial),
+    then on "go" times it on all host threads and sends the figures back.
+    kind "ppi": the reference's PPI tree (open-harmonia/src): point search
+    (BPlusTree::search), range scans (the parallel walk of cpu-range.cpp) and
+    one update epoch of 4096K keys (insert_parallel_Newupdate_batch).  kind
+    "cfb": its pointer B+tree at order 128 (open-harmonia/regular_bpt):
+    find()."""
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)  # the reference prints from its update path
+    sys.path.insert(0, ROOT)
+    from harmonia_b200 import datagen as dg
+    from oracle import pyoracle as po
+
+    n = 1 << keys_log2
+    keys = dg.gen_keys(n, 1)
+    vals = dg.values_for(keys)
+    t0 = time.time()
+    tree = po.RefTree(keys, vals) if kind == "ppi" else po.CfbTree(keys, vals)
+    build_s = time.time() - t0
+    conn.send({"built_s": build_s})
+    if conn.recv() != "go":
+        return
+    threads = os.cpu_count() or 1
+    m = 1 << queries_log2
+    q = dg.gen_point_queries(keys, m, hit, 2)
+
+    def median_s(fn, reps=3):
+        ts = []
+        for _ in range(reps):
+            a = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - a)
+        return statistics.median(ts)
+
+    tree.search(q[: 1 << 20], threads)  # warm
+    sec = median_s(lambda: tree.search(q, threads))
+    res = {"build_s": round(build_s, 1), "cores": threads,
+           "search": {"value": round(m / sec / 1e6, 3), "unit": UNIT, "ms_per_step": round(sec * 1e3, 1),
+                      "sample": f"the whole {m}-query batch, median of 3"}}
+    if kind == "ppi":
+        st, ln = dg.gen_ranges(1 << 20, 1, 256, seed=12)
+        rec, _ = tree.range_timed(st, ln, threads)
+        sec = median_s(lambda: tree.range_timed(st, ln, threads))
+        res["range"] = {"value": round(len(st) / sec / 1e6, 3), "unit": "Mranges/s", "ms_per_step": round(sec * 1e3, 1),
+                        "records_per_s_m": round(rec / sec / 1e6, 1),
+                        "sample": "2^20 ranges of 1..256 records, the parallel walk of cpu-range.cpp, median of 3"}
+        bk, bv = dg.gen_upserts(keys, 4 << 20, 0.05, 21)
+        a = time.perf_counter()
+        tree.upsert(bk, bv)
+        sec = time.perf_counter() - a
+        res["upsert"] = {"value": round(len(bk) / sec / 1e6, 3), "unit": "Mkeys/s", "ms_per_step": round(sec * 1e3, 1),
+                         "sample": "one insert_parallel_Newupdate_batch epoch of 4096K keys (5% new), once"}
+    conn.send(res)
+
+
+class CpuReference:
+    """The spawned helpers of the reference CPU figures (see
+    _cpu_reference_worker); started before any CUDA call."""
+
+    def __init__(self, args):
+        import multiprocessing as mp
+
+        from oracle import pyoracle as po
+
+        self.procs = {}
+        ctx = mp.get_context("spawn")
+        kinds = []
+        if po.ref_available():
+            kinds.append("ppi")
+        if po.cfb_available() and args.fanout == 64:
+            kinds.append("cfb")
+        for kind in kinds:
+            a, b = ctx.Pipe()
+            p = ctx.Process(target=_cpu_reference_worker,
+                            args=(b, kind, args.keys_log2, args.queries_log2, args.hit), daemon=True)
+            p.start()
+            self.procs[kind] = (p, a)
+
+    def run(self, timeout_s: float = 600.0) -> dict:
+        """Waits for the builds, times every tree (one after another, so each
+        has all host threads), returns {kind: figures}."""
+        out = {}
+        for kind, (p, conn) in self.procs.items():
+            try:
+                if not conn.poll(timeout_s):
+                    raise TimeoutError("reference build did not finish")
+                conn.recv()
+                conn.send("go")
+                if not conn.poll(timeout_s):
+                    raise TimeoutError("reference timing did not finish")
+                out[kind] = conn.recv()
+            except Exception as e:  # reported in the line, the bench goes on
+                out[kind] = {"unavailable": repr(e)}
+            p.join(5)
+            if p.is_alive():
+                p.kill()
+        return out
 
 
 def cpu_baseline_port(keys_sorted, vals_sorted, q, seconds: float = 10.0):
@@ -200,65 +311,147 @@ def cpu_baseline_port(keys_sorted, vals_sorted, q, seconds: float = 10.0):
                       f"search (oracle/hm_oracle.c), OpenMP over {cores} threads"}
 
 
+def _digest(*arrays) -> str:
+    """SHA-256 over the little-endian int64 bytes of the arrays (the golden
+    fixtures' digest)."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for x in arrays:
+        h.update(np.ascontiguousarray(np.asarray(x), dtype="<i8").tobytes())
+    return h.hexdigest()
+
+
+def _golden(name):
+    """An entry of tests/golden/golden.json (digests of the reference CPU
+    tree's outputs on these seeded workloads), or None."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+            return json.load(f).get(name)
+    except Exception:
+        return None
+
+
 def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
     """512 batches with sizes log-uniform in [1K, 4M], half uniform (90% hits),
-    half Zipf(0.99) over key rank: one plain launch per batch vs the whole set
-    in one captured CUDA graph (joint pre-sort + bucket join or search)."""
+    half Zipf(0.99) over key rank (datagen.gen_uneven_batches): one untuned
+    launch per batch, the tuned hm_search once per batch, and the whole set in
+    one captured CUDA graph (joint pre-sort + bucket join or search).  Every
+    batch's results are checked against the reference's digests."""
     import torch
     from harmonia_b200 import datagen as dg
 
     nb = 512
-    r = dg.splitmix64(np.arange(nb, dtype=np.uint64) + np.uint64(seed) * np.uint64(1 << 40))
-    u = (r >> np.uint64(11)).astype(np.float64) / float(1 << 53)
-    sizes = np.exp(np.log(1024) + u * (np.log(4 << 20) - np.log(1024))).astype(np.int64)
-    pool_n = 1 << 24
-    pool_u = torch.from_numpy(dg.gen_point_queries(keys, pool_n, 0.9, seed + 1)).to(dev)
-    pool_z = torch.from_numpy(dg.gen_zipf_queries(sk, pool_n, 0.99, seed + 2)).to(dev)
+    sizes, hq = dg.gen_uneven_batches(keys, sk, nb, seed)
     total = int(sizes.sum())
-    allq = torch.empty(total, dtype=torch.int64, device=dev)
-    allo = torch.empty(total, dtype=torch.int64, device=dev)
-    batches, o = [], 0
-    for b in range(nb):
-        m = int(sizes[b])
-        pool = pool_u if b % 2 == 0 else pool_z
-        start = int(r[b] % np.uint64(pool_n))
-        idx = (torch.arange(m, device=dev) + start) % pool_n
-        allq[o:o + m] = pool[idx]
-        batches.append((allq[o:o + m], allo[o:o + m]))
-        o += m
-    del pool_u, pool_z
+    ends = np.concatenate([[0], np.cumsum(sizes)])
+    allq = torch.from_numpy(hq).to(dev)
+    allo = torch.empty_like(allq)
+    del hq
+    batches = [(allq[ends[b]:ends[b + 1]], allo[ends[b]:ends[b + 1]]) for b in range(nb)]
     cfg = tree.config()
-    tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0, join=2)
 
-    def plain():
+    def per_batch():
         for q, out in batches:
             tree.search(q, out)
 
+    tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0, join=2)
     for _ in range(warmup):
-        plain()
-    plain_ms = timed(steps, plain)
+        per_batch()
+    plain_ms = timed(steps, per_batch)
     tree.set_search_config(**{k: cfg[k] for k in ("group_width", "queries_per_group", "sort_bits", "cache_hints",
                                                    "join")})
+    for _ in range(warmup):
+        per_batch()
+    tuned_ms = timed(steps, per_batch)
     plan = tree.plan(batches)
     for _ in range(warmup):
         plan.launch()
     plan_ms = timed(steps, plan.launch)
-    # spot check the last step's results of a few batches against the workload's own values
-    for b in (0, 1, nb // 2, nb - 1):
-        q, out = batches[b]
-        qq = q[:2048].cpu().numpy()
-        pos = np.searchsorted(sk, qq).clip(max=len(sk) - 1)
-        exp = np.where(sk[pos] == qq, dg.values_for(qq), -1)
-        assert (out[:2048].cpu().numpy() == exp).all(), "batched results are wrong"
+    g = _golden("c4_batches")
+    res = allo.cpu().numpy()
+    if g and g["nb"] == nb and g["seed"] == seed and g["queries"] == total:
+        bad = [b for b in range(nb) if _digest(res[ends[b]:ends[b + 1]]) != g["batch_digests"][b]]
+        assert not bad, f"batched results differ from the reference in batches {bad[:8]}"
+        check = "every batch's results equal the reference's (golden c4_batches digests)"
+    else:  # spot check: a loaded key's value is splitmix64(key) >> 1, a miss is -1
+        for b in (0, 1, nb // 2, nb - 1):
+            qq = batches[b][0][:2048].cpu().numpy()
+            pos = np.searchsorted(sk, qq).clip(max=len(sk) - 1)
+            exp = np.where(sk[pos] == qq, dg.values_for(qq), -1)
+            assert (res[ends[b]:ends[b] + len(qq)] == exp).all(), "batched results are wrong"
+        check = "spot check of 4 batches"
     plan.close()
     return {"batches": nb, "queries": total, "min_batch": int(sizes.min()), "max_batch": int(sizes.max()),
+            "check": check,
             "plain_per_batch": {"value": round(total / plain_ms / 1e3, 1), "unit": UNIT,
                                 "ms_per_step": round(plain_ms, 3),
                                 "what": "one search launch per batch, unsorted, group width 4, 2 queries/group"},
+            "tuned_per_batch": {"value": round(total / tuned_ms / 1e3, 1), "unit": UNIT,
+                                "ms_per_step": round(tuned_ms, 3),
+                                "what": "hm_search with the tuned configuration once per batch (pre-sort and "
+                                        "bucket join where the automatic choice takes them), no graph"},
             "graph": {"value": round(total / plan_ms / 1e3, 1), "unit": UNIT, "ms_per_step": round(plan_ms, 3),
                       "what": "the 512 batches in one captured CUDA graph: joint 16-bit pre-sort reading the "
                               "batches in place, bucket join, inverse pre-sort writing each batch's output"},
-            "speedup": round(plain_ms / plan_ms, 3)}
+            "speedup": round(plain_ms / plan_ms, 3), "speedup_vs_tuned_per_batch": round(tuned_ms / plan_ms, 3)}
+
+
+def upsert_epochs(keys, dev, steps, peak):
+    """One update epoch of 4096K keys on the 2^26-key tree (5% new keys, the
+    rest existing with value key-1: the paper's batched-update config),
+    applied by hm_upsert_batch from device buffers to a freshly loaded tree per
+    step (CUDA events around the call; the load is not timed).  Two layouts:
+    12 of 16 leaf slots filled (new keys merge in place) and full leaves
+    (overflowing leaves rebalance their subtree or the tree is rebuilt).
+    Roofline of the in-place epoch: B_u = 16 + 128 + 2 x 256 B per touched
+    leaf / updates per touched leaf (key and value in, the descent's leaf
+    line, each touched leaf row read and written once)."""
+    import torch
+    from harmonia_b200 import BPlusTree, datagen as dg
+
+    bk, bv = dg.gen_upserts(keys, 4 << 20, 0.05, 21)
+    d_keys = torch.from_numpy(keys).to(dev)
+    d_vals = torch.from_numpy(dg.values_for(keys)).to(dev)
+    d_bk, d_bv = torch.from_numpy(bk).to(dev), torch.from_numpy(bv).to(dev)
+    g = _golden("c2_upsert_4096k")
+    out = {"keys_per_epoch": len(bk), "new_frac": 0.05}
+    sk = np.sort(keys)
+    for fill, name in ((12, "leaf_fill_12"), (16, "full_leaves")):
+        times = []
+        for i in range(1 + steps):
+            t = BPlusTree.bulk_load(d_keys, d_vals, leaf_fill=fill)
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            t.upsert(d_bk, d_bv)
+            b.record()
+            torch.cuda.synchronize()
+            if i > 0:
+                times.append(a.elapsed_time(b))
+            if i == steps and g:
+                ek, ev = t.export()
+                assert _digest(ek, ev) == g["export_digest"], "contents after the epoch differ from the reference"
+            t.close()
+        ms = statistics.median(times)
+        r = {"value": round(len(bk) / ms / 1e3, 1), "unit": "Mkeys/s", "ms_per_step": round(ms, 3),
+             "what": f"hm_upsert_batch, 4096K keys, tree bulk-loaded with {fill} keys per 16-key leaf, median of {steps}"}
+        if fill == 12:
+            n_leaf = -(-len(keys) // fill)
+            qd, rem = divmod(len(keys), n_leaf)
+            rank = np.searchsorted(sk, bk, side="right") - 1
+            rank = rank.clip(min=0)
+            cut = rem * (qd + 1)
+            leaf = np.where(rank < cut, rank // (qd + 1), rem + (rank - cut) // max(qd, 1))
+            touched = len(np.unique(leaf))
+            bu = 16 + 128 + 2 * 256 * touched / len(bk)
+            ach = bu * len(bk) / (ms * 1e-3) / 1e9
+            r["roofline"] = {"bound": "hbm", "algorithmic_bytes_per_update": round(bu, 1), "touched_leaves": touched,
+                             "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4)}
+        out[name] = r
+    out["check"] = "contents after the epoch equal the reference's (golden c2_upsert_4096k)" if g else "none"
+    return out
 
 
 def fanout_128(keys, q, d_q, dev, timed, steps, warmup, exp):
@@ -342,16 +535,39 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
             bv = np.concatenate([dg.values_for(nk), ek - 1])
             return ("u", srv.upsert(bk, bv), 0, k)
 
-        # capacity: the same mix submitted back to back
-        cap_n = 400
-        cap_kinds, cap_sizes = rng.random(cap_n), sizes(cap_n)
+        # capacity: the seeded request stream (datagen.gen_serving_stream, the
+        # same mix) submitted back to back; every read and the contents after
+        # it are checked against the reference replaying it in order
+        stream = dg.gen_serving_stream(keys, 400, seed)
+        cap_n = len(stream)
         t0 = time.perf_counter()
-        tks = [submit(u, int(m)) for u, m in zip(cap_kinds, cap_sizes)]
+        tks = []
+        for req in stream:
+            if req[0] == "search":
+                tks.append(srv.search(req[1]))
+            elif req[0] == "range":
+                tks.append(srv.range(req[1], req[2]))
+            else:
+                tks.append(srv.upsert(req[1], req[2]))
         for tk in tks:
-            tk[1].wait()
+            tk.wait()
         cap_wall = time.perf_counter() - t0
         cap_rps = cap_n / cap_wall
         cap_qps = srv.stats()["queries"] / cap_wall
+        g = _golden("c5_serving_replay")
+        if g and g["n"] == n and g["count"] == cap_n and g["seed"] == seed:
+            reads = []
+            for req, tk in zip(stream, tks):
+                if req[0] == "search":
+                    reads.append(_digest(tk._result()))
+                elif req[0] == "range":
+                    reads.append(_digest(*tk._result()))
+            assert reads == g["read_digests"], "serving reads differ from the reference replay"
+            ek, ev = tree.export()
+            assert _digest(ek, ev) == g["export_digest"], "contents after the stream differ from the reference"
+            out["check"] = ("the capacity stream's reads and the contents after it equal the reference replaying "
+                            "it in order (golden c5_serving_replay)")
+        del stream, tks
         for frac in loads:
             rate = frac * cap_rps  # requests per second
             srv.reset_stats()
@@ -396,6 +612,9 @@ def main():
     ws, rank, local = dist_init()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
+    # the reference's CPU trees build in helper processes while the GPU legs
+    # run (spawned before any CUDA call)
+    cpu_ref = CpuReference(args) if (rank == 0 and ws == 1 and args.extras) else None
 
     import torch
     import torch.distributed as dist
@@ -581,12 +800,36 @@ def main():
            "d2h_bytes_per_step": m * 8, "ms_per_step": round(e2e_ms, 3),
            "what": "BPlusTree.search on pinned host buffers: chunked H2D, search, D2H through the C ABI"}
 
+    if args.extras and args.fanout == 64:
+        extras["upsert"] = upsert_epochs(keys, dev, 3, peak)
+
     if args.extras and rank == 0:
         extras["serving"] = serving_loads(dev)
 
-    cpu = None
+    cpu = cpu_port = None
     if rank == 0 and ws == 1:
-        cpu = cpu_baseline_port(sk, dg.values_for(sk), q, seconds=8.0)
+        cpu_port = cpu_baseline_port(sk, dg.values_for(sk), q, seconds=5.0)
+        cpu = cpu_port
+    if cpu_ref is not None:
+        figs = cpu_ref.run()
+        ppi, cfb = figs.get("ppi", {}), figs.get("cfb", {})
+        if "search" in ppi:
+            f = ppi["search"]
+            cpu = {"value": f["value"], "unit": UNIT, "cores": ppi["cores"], "kind": "reference",
+                   "sample": f"{f['sample']}: OpenMP BPlusTree::search of the reference's PPI tree "
+                             f"(oracle/_ref, open-harmonia/src) over {ppi['cores']} threads; tree build "
+                             f"{ppi['build_s']} s excluded"}
+        elif ppi:
+            cpu_port["reference"] = ppi
+        if "range" in ppi and "skewed_range" in extras:
+            extras["skewed_range"]["range"]["cpu_reference"] = dict(ppi["range"], cores=ppi["cores"])
+        if "upsert" in ppi and "upsert" in extras:
+            extras["upsert"]["cpu_reference"] = dict(ppi["upsert"], cores=ppi["cores"])
+        if "fanout_128" in extras:
+            extras["fanout_128"]["cpu_reference"] = (
+                dict(cfb["search"], cores=cfb["cores"], build_s=cfb["build_s"],
+                     what="find() of the reference's pointer B+tree at order 128 (open-harmonia/regular_bpt)")
+                if "search" in cfb else cfb)
 
     if rank == 0:
         line = {
@@ -594,9 +837,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic (seeded splitmix64 keys/queries)",
-            "config": {"workload": f"point search, 2^{args.keys_log2}-key tree, fanout {args.fanout}, "
-                                   f"leaf {args.leaf_cap}, one 2^{args.queries_log2}-query batch, "
-                                   f"{int(args.hit * 100)}% hits",
+            "config": {"workload": workload_name(args),
+                       "layout": f"fanout {args.fanout} inner rows, {args.leaf_cap}-key leaf records",
                        "l2": "inputs larger than L2 (2^24 x 8 B queries + tree of "
                              f"{info.device_bytes / 2**30:.2f} GiB), no flush",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
@@ -611,6 +853,7 @@ def main():
             "roofline": roofline,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "cpu_baseline_port": cpu_port,
         }
         line.update(extras)
         if "plain" in extras:

@@ -46,10 +46,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase of bar with the given parity; false if the
-// limit was reached.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity = 0) {
-  for (long i = 0; i < kSpinLimit; i++)
+// Bounded wait for the phase of bar with the given parity: at most `polls`
+// polls; false if the limit was reached.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity = 0, long polls = kSpinLimit) {
+  for (long i = 0; i < polls; i++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

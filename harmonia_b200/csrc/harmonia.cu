@@ -1019,6 +1019,12 @@ int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n_, hm_config *best)
   return rc ? rc : hm_sync(t, 0);
 }
 
+int hm_set_wait_limit(hm_tree *t, int64_t polls) {
+  if (!t || polls < 0) return HM_EINVAL;
+  t->wait_polls = polls;
+  return HM_OK;
+}
+
 int hm_profile(hm_tree *t, int enable) {
   if (!t) return HM_EINVAL;
   t->prof = enable != 0;

@@ -61,6 +61,7 @@ struct DevTree {
   int32_t smem_nodes;  // top nodes staged in shared memory (a BFS prefix)
   int32_t smem_levels;
   int32_t cache_hints; // 1: L2 evict_last for inner rows, evict_first for leaves
+  int64_t wait_polls;  // polls of the first bounded wait for the staged top levels
 };
 
 #ifdef __CUDACC__
@@ -144,6 +145,7 @@ struct hm_tree {
   mutable int join_leafb_bits = 0;
   mutable cudaEvent_t join_leafb_ready = nullptr;
   int64_t join_tuned_min = INT64_MAX;  // smallest batch the autotuner saw the join win
+  int64_t wait_polls = int64_t(1) << 24;  // hm_set_wait_limit
   // comparison baseline (hm_search_baseline): children ids per inner node,
   // child_ids_ready recorded after the kernel that filled them
   int32_t *child_ids = nullptr;
@@ -228,6 +230,7 @@ struct hm_tree {
     d.smem_nodes = smem_nodes;
     d.smem_levels = smem_levels;
     d.cache_hints = cfg.cache_hints;
+    d.wait_polls = wait_polls;
     return d;
   }
 };

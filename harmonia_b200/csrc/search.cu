@@ -268,9 +268,9 @@ __global__ void __launch_bounds__(kThreads, (Q <= 2 ? HM_SEARCH_MINB : 1)) searc
       bulk_g2s(spref, t.prefix, pref_bytes, bar);
     }
     __syncthreads();
-    if (!mbar_wait_bounded(bar)) {
+    if (!mbar_wait_bounded(bar, 0, t.wait_polls)) {
       if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
-      mbar_wait_bounded(bar);  // let the copy land before the CTA exits
+      mbar_wait_bounded(bar);  // let the copy land (default bound) before the CTA exits
       return;
     }
   }

@@ -391,8 +391,13 @@ void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
   hm_tree *t = sv->t;
   int64_t n = 0;
   for (Req *q : ups) n += (int64_t)q->r.n;
+  // A slot retired after a device timeout may still have kernels reading the
+  // tree on its stream: no epoch may change the tree (in place, or by a
+  // rebuild that frees the old arrays) under them, so writes fail from then on.
+  bool retired = false;
+  for (auto &x : sv->slots) retired |= x.kind == -2;
   Slot *fs = free_slot_of(sv);
-  if (!fs) {  // every slot retired after device timeouts
+  if (!fs || retired) {
     for (Req *q : ups) finish(sv, q, HM_ETIMEOUT);
     return;
   }

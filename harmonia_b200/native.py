@@ -24,7 +24,7 @@ HM_UPSERT_REF_KEY_MINUS_1 = 1
 # Every symbol include/harmonia.h declares.
 EXPORTS = (
     "hm_config_default", "hm_bulk_load", "hm_search", "hm_search_batches", "hm_range",
-    "hm_range_between",    "hm_upsert_batch", "hm_export", "hm_tree_get_info", "hm_set_search_config",
+    "hm_range_between", "hm_set_wait_limit",    "hm_upsert_batch", "hm_export", "hm_tree_get_info", "hm_set_search_config",
     "hm_get_config", "hm_autotune", "hm_sync", "hm_free", "hm_strerror", "hm_launch_count",
     "hm_profile", "hm_profile_read", "hm_plan_create", "hm_plan_launch", "hm_plan_free",
     "hm_search_noalloc", "hm_server_config_default", "hm_server_start", "hm_server_submit",
@@ -104,6 +104,7 @@ def lib() -> ctypes.CDLL:
     L.hm_get_config.argtypes = [P, ctypes.POINTER(Config)]
     L.hm_autotune.argtypes = [P, P, SZ, ctypes.POINTER(Config)]
     L.hm_sync.argtypes = [P, P]
+    L.hm_set_wait_limit.argtypes = [P, ctypes.c_int64]
     L.hm_free.argtypes = [P]
     L.hm_strerror.argtypes = [I]
     L.hm_strerror.restype = ctypes.c_char_p

@@ -299,6 +299,11 @@ class BPlusTree:
         check(lib().hm_profile_read(self._h, arr, 8, ctypes.byref(n)), "hm_profile_read")
         return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms)) for i in range(min(n.value, 8))}
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls of the search kernel's bounded wait for its staged top levels
+        (default 2^24); 0 makes every such wait give up (HM_ETIMEOUT)."""
+        check(lib().hm_set_wait_limit(self._h, int(polls)), "hm_set_wait_limit")
+
     def sync(self, stream=None) -> None:
         check(lib().hm_sync(self._h, _stream_ptr(stream)), "hm_sync")
 

@@ -212,6 +212,16 @@ int hm_get_config(const hm_tree *t, hm_config *cfg);
  * and open-harmonia/tests/bit-prefix-sort-8thread.sh. */
 int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n, hm_config *best);
 
+/* Polls a search kernel makes while it waits for the top levels it stages in
+ * shared memory, before it gives up, records HM_ETIMEOUT (reported by
+ * hm_sync) and returns without results (default 2^24, far above the
+ * microseconds a copy takes).  A CTA that gave up still waits, with the
+ * default bound, for its copy to land before it exits.  For tests of the
+ * timeout path: 0 makes every staged wait give up at once.  Not thread-safe
+ * with calls in flight on the tree.  No counterpart in the reference, whose
+ * kernels have no bounded waits. */
+int hm_set_wait_limit(hm_tree *t, int64_t polls);
+
 /* Waits for the tree's outstanding work on stream s and returns any error a
  * kernel recorded (HM_ETIMEOUT for a bounded wait that gave up). */
 int hm_sync(hm_tree *t, hm_stream s);
@@ -251,7 +261,9 @@ typedef struct {
   int max_queue;               /* pending requests before HM_EBUSY (default 65536) */
   int streams;                 /* launches in flight (default 3) */
   int64_t max_launch_queries;  /* coalescing cap per launch (default 2^22) */
-  int64_t device_wait_limit_ms; /* a launch unfinished after this fails with HM_ETIMEOUT (default 30000) */
+  int64_t device_wait_limit_ms; /* a launch unfinished after this fails with HM_ETIMEOUT and its slot
+                                   is retired; while any slot is retired, upserts and deletes fail
+                                   with HM_ETIMEOUT (its kernels may still read the tree) (default 30000) */
 } hm_server_config;
 
 typedef struct {

@@ -19,6 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "libhmoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libhmref.so")
+CFB_SO = os.path.join(HERE, "_ref", "libhmref_cfb.so")
 MAX_KEY = 2**63 - 1
 
 _P = ctypes.c_void_p
@@ -224,6 +225,8 @@ def _ref_lib():
         lib.hmref_range.argtypes = [_P, _P, _P, _L, _P, _P, _P, _L]
         lib.hmref_range.restype = _L
         lib.hmref_range_between.argtypes = [_P, _P, _P, _L, _P, _P, _P, _L, ctypes.c_int]
+        lib.hmref_range_timed.argtypes = [_P, _P, _P, _L, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+        lib.hmref_range_timed.restype = _L
         lib.hmref_range_between.restype = _L
         lib.hmref_upsert.argtypes = [_P, _P, _P, _L, _L, _L]
         lib.hmref_upsert.restype = ctypes.c_int
@@ -264,6 +267,16 @@ class RefTree:
         tot = _ref_lib().hmref_range(self.h, _ptr(start), _ptr(length), n, _ptr(off), _ptr(ok), _ptr(ov), cap)
         return off, ok[:tot], ov[:tot]
 
+    def range_timed(self, start, length, threads: int = 0):
+        """The range walk over all queries in parallel (OpenMP, as the
+        reference's CPU range experiment runs it), without compaction:
+        returns (records, checksum)."""
+        start = np.ascontiguousarray(start, dtype=np.int64)
+        length = np.ascontiguousarray(length, dtype=np.int32)
+        cs = ctypes.c_longlong()
+        tot = _ref_lib().hmref_range_timed(self.h, _ptr(start), _ptr(length), len(start), threads, ctypes.byref(cs))
+        return int(tot), int(cs.value)
+
     def range_between(self, start, end, walk: bool = False):
         """Inclusive ranges by BPlusTree::range_search: every record with
         start[i] <= key <= end[i] (offsets, keys, values, compacted).  After
@@ -297,3 +310,43 @@ class RefTree:
             if m >= 0:
                 return k[:m], v[:m]
             cap *= 4
+
+
+_cfb = None
+
+
+def cfb_available() -> bool:
+    return os.path.exists(CFB_SO)
+
+
+def _cfb_lib():
+    global _cfb
+    if _cfb is None:
+        lib = ctypes.CDLL(CFB_SO)
+        lib.hmcfb_order.restype = ctypes.c_int
+        lib.hmcfb_build.argtypes = [_P, _P, _L]
+        lib.hmcfb_build.restype = _P
+        lib.hmcfb_search.argtypes = [_P, _P, _L, _P, ctypes.c_int]
+        _cfb = lib
+    return _cfb
+
+
+class CfbTree:
+    """The reference's pointer B+tree at order 128 (open-harmonia/regular_bpt),
+    built by insert() in the given key order; search is its find()."""
+
+    def __init__(self, keys, vals):
+        self._k = np.ascontiguousarray(keys, dtype=np.int64)
+        self._v = np.ascontiguousarray(vals, dtype=np.int64)
+        self.h = _cfb_lib().hmcfb_build(_ptr(self._k), _ptr(self._v), len(self._k))
+
+    @property
+    def order(self) -> int:
+        return _cfb_lib().hmcfb_order()
+
+    def search(self, q, threads: int = 0) -> np.ndarray:
+        q = np.ascontiguousarray(q, dtype=np.int64)
+        out = np.empty_like(q)
+        _cfb_lib().hmcfb_search(self.h, _ptr(q), len(q), _ptr(out), threads)
+        return out
+

@@ -53,6 +53,39 @@ BLeaf_node *leaf_for(BPlusTree *t, Inner_node *last, long long key,
   return t->getBLeafNodeByIdx(idx - t->getInnerSize_wo_last_inner_node());
 }
 
+// The walk of hmref_range for one query: up to `want` records with key >=
+// start, handed to emit(key, value); returns how many.
+template <typename Emit>
+long range_walk(BPlusTree *t, long long start, long want, Emit emit) {
+  if (want <= 0 || start == Max_Key) return 0;
+  Inner_node *last = t->search_last_level_inner_node_PPItree_Newupdate(start);
+  int relist_idx = 0;
+  BLeaf_node *node = leaf_for(t, last, start, relist_idx);
+  int idx = node->findKeyLowerBound(relist_idx, start);
+  if (idx < 0) {  // nothing >= start in this record list
+    idx = 0;
+    relist_idx++;
+  }
+  long got = 0;
+  while (node != nullptr && got < want) {
+    if (relist_idx >= node->used_relist_slot_num) {
+      node = node->next;
+      relist_idx = 0;
+      idx = 0;
+      continue;
+    }
+    if (idx >= node->size[relist_idx]) {
+      relist_idx++;
+      idx = 0;
+      continue;
+    }
+    if (!emit(node->relist[relist_idx].r[idx].r_key, node->relist[relist_idx].r[idx].val)) return -1;
+    got++;
+    idx++;
+  }
+  return got;
+}
+
 }  // namespace
 
 extern "C" {
@@ -90,6 +123,31 @@ void hmref_search(void *hp, const long long *q, long n, long long *out,
   }
 }
 
+// Timing form of the range scan, as the reference's CPU range experiment
+// runs it (OpenMP over blocks of SWP_P2 = 1000 queries, cpu-range.cpp:80-88):
+// every query walks its records into a per-thread buffer (the reference
+// fills per-query result slots); returns the record count and a checksum
+// of the keys and values so the walk is not optimised away.
+long hmref_range_timed(void *hp, const long long *start, const int *len, long n, int threads,
+                       long long *checksum) {
+  BPlusTree *t = static_cast<RefTree *>(hp)->ppi;
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+  long total = 0;
+  long long sum = 0;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1000) reduction(+ : total, sum)
+  for (long i = 0; i < n; i++) {
+    long long acc = 0;
+    const long got = range_walk(t, start[i], len[i], [&](long long k, long long v) {
+      acc += k ^ v;
+      return true;
+    });
+    total += got;
+    sum += acc;
+  }
+  if (checksum) *checksum = sum;
+  return total;
+}
+
 // Range: for query i, the first len[i] records with key >= start[i] in
 // ascending key order (fewer when the key space ends).  offsets has n+1
 // entries (exclusive scan of the per-query counts).  Returns the total number
@@ -101,36 +159,14 @@ long hmref_range(void *hp, const long long *start, const int *len, long n,
   long total = 0;
   for (long i = 0; i < n; i++) {
     offsets[i] = total;
-    long want = len[i] > 0 ? len[i] : 0;
-    if (want == 0 || start[i] == Max_Key) continue;
-    Inner_node *last = t->search_last_level_inner_node_PPItree_Newupdate(start[i]);
-    int relist_idx = 0;
-    BLeaf_node *node = leaf_for(t, last, start[i], relist_idx);
-    int idx = node->findKeyLowerBound(relist_idx, start[i]);
-    if (idx < 0) {  // nothing >= start in this record list
-      idx = 0;
-      relist_idx++;
-    }
-    long got = 0;
-    while (node != nullptr && got < want) {
-      if (relist_idx >= node->used_relist_slot_num) {
-        node = node->next;
-        relist_idx = 0;
-        idx = 0;
-        continue;
-      }
-      if (idx >= node->size[relist_idx]) {
-        relist_idx++;
-        idx = 0;
-        continue;
-      }
-      if (total >= cap) return -1;
-      okeys[total] = node->relist[relist_idx].r[idx].r_key;
-      ovals[total] = node->relist[relist_idx].r[idx].val;
+    const long got = range_walk(t, start[i], len[i], [&](long long k, long long v) {
+      if (total >= cap) return false;
+      okeys[total] = k;
+      ovals[total] = v;
       total++;
-      got++;
-      idx++;
-    }
+      return true;
+    });
+    if (got < 0) return -1;
   }
   offsets[n] = total;
   return total;

@@ -23,14 +23,20 @@ def big():
     return keys, np.sort(keys)
 
 
-@pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (128, 16), (64, 64)])
-def test_c2_point_full_size(big, fanout, leaf_cap):
+@pytest.mark.parametrize("fanout,leaf_cap,smem", [(64, 16, None), (128, 16, None), (64, 64, None),
+                                                  (64, 16, 256), (64, 16, 200 * 1024)])
+def test_c2_point_full_size(big, fanout, leaf_cap, smem):
+    """smem: the budget for top levels staged in shared memory (None: the
+    default, two levels at this size; 256 B: none; 200 KiB: still two, the
+    third level alone is 600 KB)."""
     keys, sk = big
     g = GOLD["c2_point"]
     q = dg.gen_point_queries(keys, g["m"], g["hit"], g["q_seed"])
     dq = torch.from_numpy(q).cuda()
     with BPlusTree.bulk_load(torch.from_numpy(keys).cuda(), torch.from_numpy(dg.values_for(keys)).cuda(),
-                             fanout=fanout, leaf_cap=leaf_cap) as t:
+                             fanout=fanout, leaf_cap=leaf_cap, smem_bytes=smem) as t:
+        if smem == 256:
+            assert t.info().smem_levels == 0
         for bits, join in ((0, 2), (8, 2), (16, 2), (0, 1)):
             t.set_search_config(sort_bits=bits, join=join)
             out = t.search(dq).cpu().numpy()

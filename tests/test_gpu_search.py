@@ -312,3 +312,47 @@ def test_pointer_baseline_matches(fanout, leaf_cap):
         t.upsert(bk, bv)
         ek, ev = po.upsert_set(sk, dg.values_for(sk), bk, bv)
         assert (t.search_pointer_baseline(dq).cpu().numpy() == po.PortTree(ek, ev).search(q)).all()
+
+
+def test_bounded_wait_gives_up_reports_timeout_and_recovers(c1):
+    """With a wait limit of 0 every CTA's wait for its staged top levels gives
+    up at once: the CTA records HM_ETIMEOUT (hm_sync reports it), waits with
+    the default bound for its copy to land, and returns without writing
+    results.  With the default limit the next search is exact again."""
+    keys, sk, t = c1
+    q = dg.gen_point_queries(keys, 1 << 16, 0.5, seed=71)
+    dq = cuda(q)
+    t.set_search_config(sort_bits=0, join=2)
+    try:
+        assert t.info().smem_levels > 0
+        out = torch.full_like(dq, -7)
+        t.set_wait_limit(0)
+        t.search(dq, out)
+        with pytest.raises(HarmoniaError) as e:
+            t.sync()
+        assert e.value.code == -7  # HM_ETIMEOUT
+        assert (out == -7).all()
+        t.set_wait_limit(1 << 24)
+        t.search(dq, out)
+        t.sync()
+        assert (out.cpu().numpy() == po.PortTree(sk, dg.values_for(sk)).search(q)).all()
+    finally:
+        t.set_wait_limit(1 << 24)
+        t.set_search_config(sort_bits=-1, join=-1)
+
+
+@pytest.mark.parametrize("smem,levels", [(256, 0), (49152, 2), (200 * 1024, 3)])
+def test_staged_top_levels_budget(smem, levels):
+    """2^18 keys: inner levels of 1, 4 and 256 rows; a 256-B budget stages
+    none, the default two, 200 KiB all three (every inner row in shared
+    memory).  Results equal the oracle at each depth, plain and pre-sorted."""
+    keys = dg.gen_keys(1 << 18, seed=72)
+    sk = np.sort(keys)
+    oracle = po.PortTree(sk, dg.values_for(sk))
+    q = dg.gen_point_queries(keys, 1 << 18, 0.6, seed=73)
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), smem_bytes=smem) as t:
+        info = t.info()
+        assert info.height == 3 and info.smem_levels == levels
+        for bits in (0, 8):
+            t.set_search_config(sort_bits=bits, join=2)
+            assert (t.search(cuda(q)).cpu().numpy() == oracle.search(q)).all(), bits

@@ -198,3 +198,18 @@ def test_range_between_port_and_reference_walk_match_reference(n):
     a = ref.range_between(st, en)
     c = po.PortTree(ek, ev).range_between(st, en)
     assert all((x == y).all() for x, y in zip(a, c))
+
+
+@pytest.mark.skipif(not po.cfb_available(), reason="fanout-128 reference library not built in this checkout")
+@pytest.mark.parametrize("n", [5, 1000, 1 << 16])
+def test_fanout128_reference_matches_port(n):
+    """The reference's pointer B+tree at order 128 (regular_bpt, find()) and
+    the fanout-128 restatement give the same point results."""
+    keys = dg.gen_keys(n, seed=500 + n)
+    vals = dg.values_for(keys)
+    cfb = po.CfbTree(keys, vals)
+    assert cfb.order == 128
+    sk = np.sort(keys)
+    q = dg.gen_point_queries(keys, 20000, 0.5, seed=n)
+    q[:3] = [sk[0], sk[-1], -7]
+    assert (cfb.search(q) == po.PortTree(sk, dg.values_for(sk), fanout=128).search(q)).all()
