@@ -270,15 +270,30 @@ class CpuReference:
             p.start()
             self.procs[kind] = (p, a)
 
+    def wait_built(self, timeout_s: float = 600.0) -> None:
+        """Waits for the builds, so the host-bound legs (host-buffer search,
+        serving) run with the host to themselves."""
+        self.built = getattr(self, "built", {})
+        for kind, (p, conn) in self.procs.items():
+            if kind in self.built:
+                continue
+            try:
+                if conn.poll(timeout_s):
+                    self.built[kind] = conn.recv()
+            except Exception:
+                pass
+
     def run(self, timeout_s: float = 600.0) -> dict:
         """Waits for the builds, times every tree (one after another, so each
         has all host threads), returns {kind: figures}."""
+        self.built = getattr(self, "built", {})
         out = {}
         for kind, (p, conn) in self.procs.items():
             try:
-                if not conn.poll(timeout_s):
-                    raise TimeoutError("reference build did not finish")
-                conn.recv()
+                if kind not in self.built:
+                    if not conn.poll(timeout_s):
+                        raise TimeoutError("reference build did not finish")
+                    self.built[kind] = conn.recv()
                 conn.send("go")
                 if not conn.poll(timeout_s):
                     raise TimeoutError("reference timing did not finish")
@@ -788,6 +803,9 @@ def main():
                                                   args.warmup)
     if args.extras and args.fanout == 64:
         extras["fanout_128"] = fanout_128(keys, q, d_q, dev, timed, args.steps, args.warmup, exp)
+
+    if cpu_ref is not None:
+        cpu_ref.wait_built()
 
     # ---- end to end through the public API with host (pinned) buffers ----
     h_q = torch.from_numpy(q).pin_memory()

@@ -336,7 +336,7 @@ SearchPlan plan_search(const hm_tree *t, int64_t n, int batches) {
     p.join = true;
     p.bits = join_bits(t);
   } else {
-    p.bits = c.sort_bits > 0 ? c.sort_bits : 0;
+    p.bits = (c.sort_bits > 0 && n >= t->presort_min) ? c.sort_bits : 0;
   }
   if (p.bits > 0) {  // grouped queries, grouped results, partition (offset mode), join
     p.scratch = 2 * (size_t)align_up(n * 8, 256) + partition_scratch_bytes(n, p.bits, true, p.batches);
@@ -608,6 +608,7 @@ int hm_set_search_config(hm_tree *t, const hm_config *cfg) {
   int rc = check_config(c);
   if (rc) return rc;
   t->cfg = c;
+  t->presort_min = 0;  // an explicit pre-sort applies at every batch size
   choose_smem_levels(t);
   return HM_OK;
 }
@@ -1002,8 +1003,11 @@ int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n_, hm_config *best)
       best_cfg = c;
     }
   }
-  // The descent settings serve every batch; the join, where it won, serves
-  // batches at least as large as the sample (the automatic choice).
+  // The descent settings serve every batch, a pre-sort only batches at least
+  // as large as the sample (it wins there; its fixed cost of about ten
+  // launches loses on small batches); the join, where it won, serves batches
+  // at least as large as the sample (the automatic choice).
+  t->presort_min = best_cfg.sort_bits > 0 ? n : 0;
   if (join_ms < best_ms) {
     best_cfg.join = -1;
     t->join_tuned_min = std::min<int64_t>(t->join_tuned_min, n);

@@ -145,6 +145,7 @@ struct hm_tree {
   mutable int join_leafb_bits = 0;
   mutable cudaEvent_t join_leafb_ready = nullptr;
   int64_t join_tuned_min = INT64_MAX;  // smallest batch the autotuner saw the join win
+  int64_t presort_min = 0;  // a tuned pre-sort applies from this batch size (0: any size)
   int64_t wait_polls = int64_t(1) << 24;  // hm_set_wait_limit
   // comparison baseline (hm_search_baseline): children ids per inner node,
   // child_ids_ready recorded after the kernel that filled them
