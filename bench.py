@@ -209,7 +209,8 @@ def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
     keys = dg.gen_keys(n, 1)
     vals = dg.values_for(keys)
     t0 = time.time()
-    tree = po.RefTree(keys, vals) if kind == "ppi" else po.CfbTree(keys, vals)
+    gpu = kind == "ppi" and po.gpu_ref_available()
+    tree = po.RefTree(keys, vals, gpu=gpu) if kind == "ppi" else po.CfbTree(keys, vals)
     build_s = time.time() - t0
     conn.send({"built_s": build_s})
     if conn.recv() != "go":
@@ -238,6 +239,27 @@ def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
         res["range"] = {"value": round(len(st) / sec / 1e6, 3), "unit": "Mranges/s", "ms_per_step": round(sec * 1e3, 1),
                         "records_per_s_m": round(rec / sec / 1e6, 1),
                         "sample": "2^20 ranges of 1..256 records, the parallel walk of cpu-range.cpp, median of 3"}
+        if gpu:  # the reference's own GPU search on this GPU, after every GPU leg of the bench
+            try:
+                g = po.RefGpuSearch(tree)
+                out, md, mc = g.search(q, reps=5)
+                g.close()
+                gold = _golden("c2_point")
+                if gold and gold["n"] == n and gold["m"] == m and gold["hit"] == hit:
+                    ok = _digest(out) == gold["digest"]
+                    check = "results equal the reference CPU tree's (golden c2_point digest)" if ok else "DIFFERS"
+                else:
+                    ok = bool((out[: 1 << 16] == tree.search(q[: 1 << 16], threads)).all())
+                    check = "results equal the reference CPU tree's on 2^16 queries" if ok else "DIFFERS"
+                res["gpu"] = {"value": round(m / md / 1e3, 1), "unit": UNIT, "ms_per_step": round(md, 4),
+                              "with_copies": {"value": round(m / mc / 1e3, 1), "unit": UNIT, "ms_per_step": round(mc, 3)},
+                              "check": check,
+                              "what": "the reference's GPU search compiled for sm_100a (open-harmonia/src/full-multi-"
+                                      "prefix-sort-8thread.cu: CUB SortPairs on bits [48,64) + the 8-thread kernel) "
+                                      "on its own PPI tree, device-resident keys, mean of 5; with_copies adds the "
+                                      "key upload and the result download (oracle/ref_gpu_driver.cu)"}
+            except Exception as e:
+                res["gpu"] = {"unavailable": repr(e)}
         bk, bv = dg.gen_upserts(keys, 4 << 20, 0.05, 21)
         a = time.perf_counter()
         tree.upsert(bk, bv)
@@ -566,9 +588,9 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
                 tks.append(srv.upsert(req[1], req[2]))
         for tk in tks:
             tk.wait()
-        cap_wall = time.perf_counter() - t0
-        cap_rps = cap_n / cap_wall
-        cap_qps = srv.stats()["queries"] / cap_wall
+        burst_wall = time.perf_counter() - t0
+        burst = {"requests": cap_n, "req_per_s": round(cap_n / burst_wall, 1),
+                 "mqps": round(srv.stats()["queries"] / burst_wall / 1e6, 1)}
         g = _golden("c5_serving_replay")
         if g and g["n"] == n and g["count"] == cap_n and g["seed"] == seed:
             reads = []
@@ -583,6 +605,19 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
             out["check"] = ("the capacity stream's reads and the contents after it equal the reference replaying "
                             "it in order (golden c5_serving_replay)")
         del stream, tks
+        # sustained capacity: the mix submitted back to back for about two
+        # seconds (a 400-request burst overstates what the loop sustains)
+        srv.reset_stats()
+        cap_n = max(2000, int(2.0 * burst["req_per_s"]))
+        cap_kinds, cap_sizes = rng.random(cap_n), sizes(cap_n)
+        t0 = time.perf_counter()
+        tks = [submit(u, int(m)) for u, m in zip(cap_kinds, cap_sizes)]
+        for tk in tks:
+            tk[1].wait()
+        cap_wall = time.perf_counter() - t0
+        cap_rps = cap_n / cap_wall
+        cap_qps = srv.stats()["queries"] / cap_wall
+        del tks
         for frac in loads:
             rate = frac * cap_rps  # requests per second
             srv.reset_stats()
@@ -606,7 +641,11 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
                                    "throughput_mqps": round(st["queries"] / wall / 1e6, 1),
                                    "p50_ms": round(st["p50_us"] / 1e3, 3), "p99_ms": round(st["p99_us"] / 1e3, 3),
                                    "max_ms": round(st["max_us"] / 1e3, 3), "launches": st["launches"],
-                                   "epochs": st["epochs"], "failed": st["failed"]}
+                                   "epochs": st["epochs"], "failed": st["failed"],
+                                   "split_ms": {k[:-3]: round(st[k] / 1e3, 3) for k in (
+                                       "queue_p50_us", "queue_p99_us", "stage_p50_us", "stage_p99_us",
+                                       "device_p50_us", "device_p99_us", "finish_p50_us", "finish_p99_us",
+                                       "epoch_drain_mean_us", "epoch_apply_mean_us")}}
         # answers in the mix: a point request's hits return splitmix64(key)>>1 or key-1 (updated)
         s_hits = [t for t in tickets if t[0] == "s"][:20]
         for kind, tk, o, m in s_hits:
@@ -614,8 +653,10 @@ def serving_loads(dev, loads=(0.25, 0.5, 0.9), seconds=2.0, seed=11):
             got = tk._result()
             ok = (got == -1) | (got == dg.values_for(q)) | (got == q - 1)
             assert ok.all(), "serving answer outside the possible values"
-        out["capacity"] = {"req_per_s": round(cap_rps, 1), "mqps": round(cap_qps / 1e6, 1),
-                           "what": "the same request mix submitted back to back; loads are fractions of it"}
+        out["capacity"] = {"req_per_s": round(cap_rps, 1), "mqps": round(cap_qps / 1e6, 1), "requests": cap_n,
+                           "what": "the request mix submitted back to back for about 2 s; loads are fractions "
+                                   "of it"}
+        out["burst"] = dict(burst, what="the 400-request seeded stream submitted back to back (the parity run)")
     tree.close()
     return out
 
@@ -841,6 +882,8 @@ def main():
             cpu_port["reference"] = ppi
         if "range" in ppi and "skewed_range" in extras:
             extras["skewed_range"]["range"]["cpu_reference"] = dict(ppi["range"], cores=ppi["cores"])
+        if "gpu" in ppi:
+            extras["reference_gpu"] = ppi["gpu"]
         if "upsert" in ppi and "upsert" in extras:
             extras["upsert"]["cpu_reference"] = dict(ppi["upsert"], cores=ppi["cores"])
         if "fanout_128" in extras:

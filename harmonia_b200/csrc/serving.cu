@@ -44,6 +44,9 @@ struct Req {
   hm_request r{};
   int status = 1;  // 1 = pending
   Clock::time_point t_submit;
+  // where a read's time goes: taken into a launch, launch enqueued (inputs
+  // staged and copied), launch seen finished on the device
+  Clock::time_point t_admit, t_enqueued, t_device_done;
   double latency_us = 0;
   size_t bytes = 0;  // device bytes the request needs while in flight
 };
@@ -86,7 +89,7 @@ class CopyPool {
     for (auto &t : th_) t.join();
     th_.clear();
   }
-  // Runs every copy (split into 1 MiB pieces) on the helpers and the calling
+  // Runs every copy (split into kPiece pieces) on the helpers and the calling
   // thread; returns when all are done.  One caller at a time.
   void run(const std::vector<CopyJob> &jobs) {
     size_t total = 0;
@@ -121,7 +124,10 @@ class CopyPool {
   }
 
  private:
-  static constexpr size_t kPiece = (size_t)1 << 20;
+  // measured on the serving mix: the dispatcher's own copies of requests
+  // below a MiB (most of them) capped its rate when only larger copies were
+  // shared out
+  static constexpr size_t kPiece = (size_t)128 << 10;
   void work() {
     std::unique_lock<std::mutex> lk(mu_);
     for (;;) {
@@ -175,20 +181,36 @@ struct hm_server {
   CopyPool copies;
   // stats
   std::vector<double> lat;
+  std::vector<double> lat_queue, lat_stage, lat_device, lat_finish;  // reads only
+  double epoch_drain_us = 0, epoch_apply_us = 0;  // summed over epochs
   uint64_t completed = 0, rejected = 0, launches = 0, epochs = 0, queries = 0, failed = 0;
   Clock::time_point t_start;
 };
 
 namespace {
 
+double us_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::micro>(b - a).count();
+}
+
 void finish(hm_server *sv, Req *q, int status) {
   q->status = status;
-  q->latency_us = std::chrono::duration<double, std::micro>(Clock::now() - q->t_submit).count();
+  const Clock::time_point now = Clock::now();
+  q->latency_us = us_between(q->t_submit, now);
+  const bool read = q->r.kind == HM_REQ_SEARCH || q->r.kind == HM_REQ_RANGE;
+  const bool timed = read && status == HM_OK && q->t_device_done >= q->t_enqueued && q->t_enqueued >= q->t_admit &&
+                     q->t_admit >= q->t_submit;
   std::lock_guard<std::mutex> lk(sv->mu);
   sv->completed++;
   if (status != HM_OK) sv->failed++;
   sv->queries += q->r.n;
   sv->lat.push_back(q->latency_us);
+  if (timed) {
+    sv->lat_queue.push_back(us_between(q->t_submit, q->t_admit));
+    sv->lat_stage.push_back(us_between(q->t_admit, q->t_enqueued));
+    sv->lat_device.push_back(us_between(q->t_enqueued, q->t_device_done));
+    sv->lat_finish.push_back(us_between(q->t_device_done, now));
+  }
   sv->cv_done.notify_all();
 }
 
@@ -353,10 +375,13 @@ bool poll_slots(hm_server *sv, int64_t wait_us) {
         sl.retired = true;
       } else if (e != cudaSuccess) {
         for (Req *q : sl.reqs) finish(sv, q, cuda_err(e));
-      } else if (sl.kind == HM_REQ_SEARCH) {
-        complete_points(sv, sl);
       } else {
-        complete_ranges(sv, sl);
+        const Clock::time_point now = Clock::now();
+        for (Req *q : sl.reqs) q->t_device_done = now;
+        if (sl.kind == HM_REQ_SEARCH)
+          complete_points(sv, sl);
+        else
+          complete_ranges(sv, sl);
       }
       {
         std::lock_guard<std::mutex> lk(sv->mu);
@@ -387,7 +412,9 @@ Slot *free_slot_of(hm_server *sv) {
 
 // Applies a run of upserts as one epoch after every earlier request finished.
 void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
+  const Clock::time_point t0 = Clock::now();
   while (slots_busy(sv)) poll_slots(sv, 1000);
+  const Clock::time_point t1 = Clock::now();
   hm_tree *t = sv->t;
   int64_t n = 0;
   for (Req *q : ups) n += (int64_t)q->r.n;
@@ -431,6 +458,8 @@ void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->epochs++;
+    sv->epoch_drain_us += us_between(t0, t1);
+    sv->epoch_apply_us += us_between(t1, Clock::now());
   }
   for (Req *q : ups) finish(sv, q, rc);
 }
@@ -499,6 +528,8 @@ void dispatcher(hm_server *sv) {
         free_slot->reserved = bytes;
         free_slot->kind = kind;
         free_slot->reqs = take;
+        const Clock::time_point now = Clock::now();
+        for (Req *q : take) q->t_admit = now;
       }
     }
     if (kind == HM_REQ_UPSERT || kind == HM_REQ_DELETE) {
@@ -510,6 +541,8 @@ void dispatcher(hm_server *sv) {
       if (x.kind >= 0 && !x.reqs.empty() && x.reqs[0] == take[0]) sl = &x;
     sl->t_launch = Clock::now();
     int rc = kind == HM_REQ_SEARCH ? launch_points(sv, *sl) : launch_ranges(sv, *sl);
+    const Clock::time_point enq = Clock::now();
+    for (Req *q : sl->reqs) q->t_enqueued = enq;
     {
       std::lock_guard<std::mutex> lk(sv->mu);
       sv->launches++;
@@ -625,7 +658,7 @@ int hm_server_start(hm_tree *t, const hm_server_config *cfg, hm_server **out) {
   }
   sv->t_start = Clock::now();
   const unsigned hw = std::thread::hardware_concurrency();
-  sv->copies.start((int)std::min(8u, std::max(1u, hw / 4)));
+  sv->copies.start((int)std::min(8u, std::max(1u, hw / 3)));
   sv->th = std::thread(dispatcher, sv);
   *out = sv;
   return HM_OK;
@@ -688,19 +721,31 @@ int hm_server_get_stats(hm_server *sv, hm_server_stats *st) {
   st->queries = sv->queries;
   st->pending = sv->queue.size();
   st->elapsed_s = std::chrono::duration<double>(Clock::now() - sv->t_start).count();
+  auto pct = [](std::vector<double> v, double p) {
+    if (v.empty()) return 0.0;
+    size_t k = (size_t)(p * (v.size() - 1) + 0.5);
+    std::nth_element(v.begin(), v.begin() + k, v.end());
+    return v[k];
+  };
   if (!sv->lat.empty()) {
-    std::vector<double> v = sv->lat;
-    auto pct = [&](double p) {
-      size_t k = (size_t)(p * (v.size() - 1) + 0.5);
-      std::nth_element(v.begin(), v.begin() + k, v.end());
-      return v[k];
-    };
-    st->p50_us = pct(0.50);
-    st->p99_us = pct(0.99);
-    st->max_us = *std::max_element(v.begin(), v.end());
+    st->p50_us = pct(sv->lat, 0.50);
+    st->p99_us = pct(sv->lat, 0.99);
+    st->max_us = *std::max_element(sv->lat.begin(), sv->lat.end());
     double s = 0;
-    for (double x : v) s += x;
-    st->mean_us = s / v.size();
+    for (double x : sv->lat) s += x;
+    st->mean_us = s / sv->lat.size();
+  }
+  st->queue_p50_us = pct(sv->lat_queue, 0.50);
+  st->queue_p99_us = pct(sv->lat_queue, 0.99);
+  st->stage_p50_us = pct(sv->lat_stage, 0.50);
+  st->stage_p99_us = pct(sv->lat_stage, 0.99);
+  st->device_p50_us = pct(sv->lat_device, 0.50);
+  st->device_p99_us = pct(sv->lat_device, 0.99);
+  st->finish_p50_us = pct(sv->lat_finish, 0.50);
+  st->finish_p99_us = pct(sv->lat_finish, 0.99);
+  if (sv->epochs) {
+    st->epoch_drain_mean_us = sv->epoch_drain_us / (double)sv->epochs;
+    st->epoch_apply_mean_us = sv->epoch_apply_us / (double)sv->epochs;
   }
   return HM_OK;
 }
@@ -709,6 +754,11 @@ int hm_server_reset_stats(hm_server *sv) {
   if (!sv) return HM_EINVAL;
   std::lock_guard<std::mutex> lk(sv->mu);
   sv->lat.clear();
+  sv->lat_queue.clear();
+  sv->lat_stage.clear();
+  sv->lat_device.clear();
+  sv->lat_finish.clear();
+  sv->epoch_drain_us = sv->epoch_apply_us = 0;
   sv->completed = sv->failed = sv->rejected = sv->launches = sv->epochs = sv->queries = 0;
   sv->t_start = Clock::now();
   return HM_OK;

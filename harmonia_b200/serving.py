@@ -33,7 +33,12 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("epochs", ctypes.c_uint64), ("queries", ctypes.c_uint64),
                 ("pending", ctypes.c_uint64), ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double),
-                ("max_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("elapsed_s", ctypes.c_double)]
+                ("max_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("elapsed_s", ctypes.c_double),
+                ("queue_p50_us", ctypes.c_double), ("queue_p99_us", ctypes.c_double),
+                ("stage_p50_us", ctypes.c_double), ("stage_p99_us", ctypes.c_double),
+                ("device_p50_us", ctypes.c_double), ("device_p99_us", ctypes.c_double),
+                ("finish_p50_us", ctypes.c_double), ("finish_p99_us", ctypes.c_double),
+                ("epoch_drain_mean_us", ctypes.c_double), ("epoch_apply_mean_us", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -270,6 +270,17 @@ typedef struct {
   uint64_t completed, failed, rejected, launches, epochs, queries, pending;
   double p50_us, p99_us, max_us, mean_us; /* submit-to-completion latency */
   double elapsed_s;
+  /* Where a read's time goes (searches and ranges completed since the last
+   * reset, p50 and p99 of each part): queue = submitted until taken into a
+   * launch (waits for slots, the memory budget and write epochs ahead of it);
+   * stage = inputs copied to pinned staging and the launch enqueued; device =
+   * enqueued until the launch is seen finished (copies and kernels); finish =
+   * results copied to the caller's buffers.  Per write epoch, the mean wait
+   * for the launches before it to finish (drain) and the mean time to apply
+   * it. */
+  double queue_p50_us, queue_p99_us, stage_p50_us, stage_p99_us;
+  double device_p50_us, device_p99_us, finish_p50_us, finish_p99_us;
+  double epoch_drain_mean_us, epoch_apply_mean_us;
 } hm_server_stats;
 
 typedef struct hm_server hm_server;

@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "libhmoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libhmref.so")
 CFB_SO = os.path.join(HERE, "_ref", "libhmref_cfb.so")
+GPU_SO = os.path.join(HERE, "_ref", "libhmref_gpu.so")
 MAX_KEY = 2**63 - 1
 
 _P = ctypes.c_void_p
@@ -209,10 +210,16 @@ def delete_set(skeys, svals, dkeys):
     return skeys[keep], svals[keep]
 
 
-def _ref_lib():
+def gpu_ref_available() -> bool:
+    return os.path.exists(GPU_SO)
+
+
+def _ref_lib(path: str = REF_SO):
     global _ref
     if _ref is None:
-        lib = ctypes.CDLL(REF_SO)
+        _ref = {}
+    if path not in _ref:
+        lib = ctypes.CDLL(path)
         lib.hmref_build.argtypes = [_P, _P, _L]
         lib.hmref_build.restype = _P
         for f in ("hmref_height",):
@@ -232,28 +239,40 @@ def _ref_lib():
         lib.hmref_upsert.restype = ctypes.c_int
         lib.hmref_export.argtypes = [_P, _P, _P, _L]
         lib.hmref_export.restype = _L
-        _ref = lib
-    return _ref
+        if path == GPU_SO:
+            lib.hmrefgpu_prepare.argtypes = [_P]
+            lib.hmrefgpu_prepare.restype = _P
+            lib.hmrefgpu_free.argtypes = [_P]
+            lib.hmrefgpu_check.argtypes = [_P, _P, _L]
+            lib.hmrefgpu_check.restype = _L
+            lib.hmrefgpu_search.argtypes = [_P, _P, _L, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                                            ctypes.POINTER(ctypes.c_float)]
+            lib.hmrefgpu_search.restype = ctypes.c_int
+        _ref[path] = lib
+    return _ref[path]
 
 
 class RefTree:
-    """The reference's PPI tree, built by inserting keys in the given order."""
+    """The reference's PPI tree, built by inserting keys in the given order.
+    gpu=True loads the library that also holds the reference's GPU search
+    (oracle/_ref/libhmref_gpu.so), for RefGpuSearch."""
 
-    def __init__(self, keys, vals):
+    def __init__(self, keys, vals, gpu: bool = False):
         self._k = np.ascontiguousarray(keys, dtype=np.int64)
         self._v = np.ascontiguousarray(vals, dtype=np.int64)
-        self.h = _ref_lib().hmref_build(_ptr(self._k), _ptr(self._v), len(self._k))
+        self.lib_path = GPU_SO if gpu else REF_SO
+        self.h = _ref_lib(self.lib_path).hmref_build(_ptr(self._k), _ptr(self._v), len(self._k))
         if not self.h:
             raise ValueError("the reference needs more than 4 keys for a PPI tree")
 
     @property
     def height(self) -> int:
-        return _ref_lib().hmref_height(self.h)
+        return _ref_lib(self.lib_path).hmref_height(self.h)
 
     def search(self, q, threads: int = 0) -> np.ndarray:
         q = np.ascontiguousarray(q, dtype=np.int64)
         out = np.empty_like(q)
-        _ref_lib().hmref_search(self.h, _ptr(q), len(q), _ptr(out), threads)
+        _ref_lib(self.lib_path).hmref_search(self.h, _ptr(q), len(q), _ptr(out), threads)
         return out
 
     def range(self, start, length):
@@ -264,7 +283,7 @@ class RefTree:
         off = np.empty(n + 1, np.int64)
         ok = np.empty(max(cap, 1), np.int64)
         ov = np.empty(max(cap, 1), np.int64)
-        tot = _ref_lib().hmref_range(self.h, _ptr(start), _ptr(length), n, _ptr(off), _ptr(ok), _ptr(ov), cap)
+        tot = _ref_lib(self.lib_path).hmref_range(self.h, _ptr(start), _ptr(length), n, _ptr(off), _ptr(ok), _ptr(ov), cap)
         return off, ok[:tot], ov[:tot]
 
     def range_timed(self, start, length, threads: int = 0):
@@ -274,7 +293,7 @@ class RefTree:
         start = np.ascontiguousarray(start, dtype=np.int64)
         length = np.ascontiguousarray(length, dtype=np.int32)
         cs = ctypes.c_longlong()
-        tot = _ref_lib().hmref_range_timed(self.h, _ptr(start), _ptr(length), len(start), threads, ctypes.byref(cs))
+        tot = _ref_lib(self.lib_path).hmref_range_timed(self.h, _ptr(start), _ptr(length), len(start), threads, ctypes.byref(cs))
         return int(tot), int(cs.value)
 
     def range_between(self, start, end, walk: bool = False):
@@ -290,7 +309,7 @@ class RefTree:
         while True:
             ok = np.empty(cap, np.int64)
             ov = np.empty(cap, np.int64)
-            tot = _ref_lib().hmref_range_between(self.h, _ptr(start), _ptr(end), n, _ptr(off), _ptr(ok),
+            tot = _ref_lib(self.lib_path).hmref_range_between(self.h, _ptr(start), _ptr(end), n, _ptr(off), _ptr(ok),
                                                  _ptr(ov), cap, 1 if walk else 0)
             if tot >= 0:
                 return off, ok[:tot], ov[:tot]
@@ -299,14 +318,14 @@ class RefTree:
     def upsert(self, keys, vals, syn_batch: int = 0, rebuild_batch: int = 0) -> None:
         keys = np.ascontiguousarray(keys, dtype=np.int64)
         vals = np.ascontiguousarray(vals, dtype=np.int64)
-        _ref_lib().hmref_upsert(self.h, _ptr(keys), _ptr(vals), len(keys), syn_batch, rebuild_batch)
+        _ref_lib(self.lib_path).hmref_upsert(self.h, _ptr(keys), _ptr(vals), len(keys), syn_batch, rebuild_batch)
 
     def export(self):
         cap = 1 << 12
         while True:
             k = np.empty(cap, np.int64)
             v = np.empty(cap, np.int64)
-            m = _ref_lib().hmref_export(self.h, _ptr(k), _ptr(v), cap)
+            m = _ref_lib(self.lib_path).hmref_export(self.h, _ptr(k), _ptr(v), cap)
             if m >= 0:
                 return k[:m], v[:m]
             cap *= 4
@@ -349,4 +368,45 @@ class CfbTree:
         out = np.empty_like(q)
         _cfb_lib().hmcfb_search(self.h, _ptr(q), len(q), _ptr(out), threads)
         return out
+
+
+class RefGpuSearch:
+    """The reference's own GPU point search (open-harmonia/src/full-multi-
+    prefix-sort-8thread.cu: CUB SortPairs on bits [48, 64) and the 8-thread
+    kernel) on a RefTree built with gpu=True, through oracle/ref_gpu_driver.cu."""
+
+    def __init__(self, tree: RefTree):
+        if tree.lib_path != GPU_SO:
+            raise ValueError("build the RefTree with gpu=True")
+        self.tree = tree
+        self.lib = _ref_lib(GPU_SO)
+        self.g = self.lib.hmrefgpu_prepare(tree.h)
+        if not self.g:
+            raise RuntimeError("hmrefgpu_prepare failed (no device, or out of memory)")
+
+    def check(self, q) -> int:
+        """Keys the kernel would search outside the tree's arrays (CPU only)."""
+        q = np.ascontiguousarray(q, dtype=np.int64)
+        return int(self.lib.hmrefgpu_check(self.tree.h, _ptr(q), len(q)))
+
+    def search(self, q, reps: int = 3):
+        """(values, mean device ms of sort + kernel, device ms with copies)."""
+        q = np.ascontiguousarray(q, dtype=np.int64)
+        out = np.full(len(q), -7, np.int64)
+        md, mc = ctypes.c_float(), ctypes.c_float()
+        rc = self.lib.hmrefgpu_search(self.g, _ptr(q), len(q), _ptr(out), reps, ctypes.byref(md), ctypes.byref(mc))
+        if rc != 0:
+            raise RuntimeError(f"hmrefgpu_search failed: {rc}")
+        return out, float(md.value), float(mc.value)
+
+    def close(self):
+        if self.g:
+            self.lib.hmrefgpu_free(self.g)
+            self.g = None
+
+
+def check_gpu_ref_batch(tree: RefTree, q) -> int:
+    """The CPU check of the reference GPU kernel's index path alone."""
+    q = np.ascontiguousarray(q, dtype=np.int64)
+    return int(_ref_lib(GPU_SO).hmrefgpu_check(tree.h, _ptr(q), len(q)))
 

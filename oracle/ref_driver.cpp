@@ -105,6 +105,8 @@ void *hmref_build(const long long *keys, const long long *vals, long n) {
 }
 
 int hmref_height(void *hp) { return static_cast<RefTree *>(hp)->ppi->getHeight(); }
+// The PPI tree itself, for the GPU comparison driver linked beside this file.
+void *hmref_ppi_tree(void *hp) { return static_cast<RefTree *>(hp)->ppi; }
 long hmref_inner_nodes(void *hp) { return static_cast<RefTree *>(hp)->ppi->getInnerSize(); }
 long hmref_big_leaves(void *hp) { return static_cast<RefTree *>(hp)->ppi->getBLeafSize(); }
 

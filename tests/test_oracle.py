@@ -213,3 +213,18 @@ def test_fanout128_reference_matches_port(n):
     q = dg.gen_point_queries(keys, 20000, 0.5, seed=n)
     q[:3] = [sk[0], sk[-1], -7]
     assert (cfb.search(q) == po.PortTree(sk, dg.values_for(sk), fanout=128).search(q)).all()
+
+
+@pytest.mark.skipif(not po.gpu_ref_available(), reason="reference GPU library not built in this checkout")
+def test_reference_gpu_library_cpu_side():
+    """The library holding the reference's GPU search also holds its CPU tree
+    (same answers as the plain reference library), and the CPU check of the
+    GPU kernel's index path accepts the seeded workloads (uniform and Zipf)."""
+    keys = dg.gen_keys(1 << 16, seed=77)
+    vals = dg.values_for(keys)
+    t = po.RefTree(keys, vals, gpu=True)
+    q = dg.gen_point_queries(keys, 1 << 16, 0.5, seed=78)
+    assert (t.search(q) == po.RefTree(keys, vals).search(q)).all()
+    assert po.check_gpu_ref_batch(t, q) == 0
+    assert po.check_gpu_ref_batch(t, dg.gen_zipf_queries(np.sort(keys), 1 << 16, 0.99, seed=79)) == 0
+    assert po.check_gpu_ref_batch(t, np.array([po.MAX_KEY], np.int64)) == 1  # never sent to the kernel
