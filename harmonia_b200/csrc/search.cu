@@ -160,6 +160,39 @@ __device__ __forceinline__ int match_slot(const int64_t *p, int64_t q, int sub, 
   return slot;
 }
 
+// Equality test over a 16-key leaf record that also loads, in the same round
+// trip, the values beside the lane's keys: the matching lane returns the
+// value (others HM_NOT_FOUND), so no dependent load follows the compare.
+#ifndef HM_LEAF_VALUES_WITH_KEYS
+#define HM_LEAF_VALUES_WITH_KEYS 0  // 1: 256 B read per leaf, one DRAM round trip fewer
+#endif
+template <int W, int LC>
+__device__ __forceinline__ int64_t match_value(const int64_t *p, int64_t q, int sub, uint64_t pol, bool *hit) {
+  constexpr int NV = LC / 2;
+  constexpr int VPL = (NV + W - 1) / W;
+  longlong2 v[VPL], w[VPL];
+#pragma unroll
+  for (int i = 0; i < VPL; i++) {
+    const int vi = sub + i * W;
+    if (NV % W == 0 || vi < NV) {
+      v[i] = ldg2(p + 2 * vi, pol);
+      w[i] = ldg2(p + LC + 2 * vi, pol);
+    } else {
+      v[i] = make_longlong2(kMaxKey, kMaxKey);
+      w[i] = make_longlong2(HM_NOT_FOUND, HM_NOT_FOUND);
+    }
+  }
+  int64_t r = HM_NOT_FOUND;
+  bool h = false;
+#pragma unroll
+  for (int i = 0; i < VPL; i++) {
+    if (v[i].x == q) { r = w[i].x; h = true; }
+    if (v[i].y == q) { r = w[i].y; h = true; }
+  }
+  *hit = h;
+  return r;
+}
+
 // Processes one tile of up to G*Q queries: q_base[i] for i in [i0, i0+G*Q) ∩ [0, n).
 template <int W, int F, int LC, int Q>
 __device__ __forceinline__ void search_tile(const DevTree &t, const int64_t *srows,
@@ -210,6 +243,28 @@ __device__ __forceinline__ void search_tile(const DevTree &t, const int64_t *sro
         node[j] = base[j] + 8 * k[j] + count_le<W, 8, false>(row + F / 8 + 8 * k[j], nav[j], sub, pol_inner);
       }
     }
+  }
+
+  if constexpr (LI == 0 && HM_LEAF_VALUES_WITH_KEYS) {
+    int64_t val[Q];
+    bool found[Q];
+#pragma unroll
+    for (int j = 0; j < Q; j++) {
+      const int64_t *row = t.leaf_rows + (int64_t)(node[j] - t.n_inner) * LROW;
+      val[j] = match_value<W, LC>(row, key[j], sub, pol_leaf, &found[j]);
+      if (key[j] == kMaxKey) found[j] = false;
+    }
+    const unsigned gm = (W == 32) ? 0xffffffffu : (((1u << W) - 1u) << (lane & ~(W - 1)));
+#pragma unroll
+    for (int j = 0; j < Q; j++) {
+      const unsigned hit = __ballot_sync(0xffffffffu, found[j]) & gm;
+      const int writer = hit ? (__ffs(hit) - 1) : (lane & ~(W - 1));
+      if (lane == writer && idx[j] < n) {
+        const int64_t o = posp ? (int64_t)__ldg(posp + idx[j]) : idx[j];
+        outp[o] = found[j] ? val[j] : (int64_t)HM_NOT_FOUND;
+      }
+    }
+    return;
   }
 
   int slot[Q];

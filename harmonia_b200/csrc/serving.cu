@@ -59,7 +59,11 @@ struct Slot {
   char *pin = nullptr;
   size_t pin_bytes = 0;
   std::vector<Req *> reqs;
-  int kind = -1;  // HM_REQ_SEARCH or HM_REQ_RANGE while busy, -1 free, -2 retired
+  // HM_REQ_SEARCH or HM_REQ_RANGE while its launch runs, -3 while the
+  // completer copies its results out, -1 free, -2 retired; only the
+  // dispatcher thread reads or writes it
+  int kind = -1;
+  int launched = -1;  // the kind of the launch being completed
   int64_t n = 0;
   size_t reserved = 0;
   bool retired = false;
@@ -178,7 +182,16 @@ struct hm_server {
   std::thread th;
   std::vector<Slot> slots;
   size_t reserved = 0;
-  CopyPool copies;
+  CopyPool copies;      // the dispatcher's copies into pinned staging
+  CopyPool copies_out;  // the completer's copies out to the callers' buffers
+  // Launches seen finished on the device go to the completer thread, which
+  // copies the results out and finishes the requests, then hands the slot
+  // back (handed_back) for the dispatcher to free; both queues under mu.
+  std::thread completer;
+  std::deque<Slot *> to_complete, handed_back;
+  std::condition_variable cv_complete;
+  bool completer_quit = false;
+  Slot epoch_slot;  // staging and stream of write epochs
   // stats
   std::vector<double> lat;
   std::vector<double> lat_queue, lat_stage, lat_device, lat_finish;  // reads only
@@ -277,7 +290,7 @@ void complete_points(hm_server *sv, Slot &sl) {
     jobs.push_back({reinterpret_cast<char *>(q->r.out), reinterpret_cast<const char *>(hout + o), q->r.n * 8});
     o += (int64_t)q->r.n;
   }
-  sv->copies.run(jobs);
+  sv->copies_out.run(jobs);
   for (Req *q : sl.reqs) finish(sv, q, HM_OK);
 }
 
@@ -357,31 +370,52 @@ void complete_ranges(hm_server *sv, Slot &sl) {
   }
 }
 
-// Completes finished launches.  With wait_us > 0, polls until at least one
-// launch finished or the time is up; a launch that has not finished within
-// the server's device wait limit is failed with HM_ETIMEOUT and its slot
-// retired (its buffers stay allocated: the stream may still own them).
+// Watches the launches in flight.  A launch seen finished goes to the
+// completer thread (its slot is "completing" until the completer hands it
+// back); slots handed back are freed here.  With wait_us > 0, polls until at
+// least one launch finished or was handed back, or the time is up.  A launch
+// that has not finished within the server's device wait limit is failed with
+// HM_ETIMEOUT and its slot retired (its buffers stay allocated: the stream may
+// still own them).
 bool poll_slots(hm_server *sv, int64_t wait_us) {
   const Clock::time_point t0 = Clock::now();
   for (;;) {
     bool any = false;
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      while (!sv->handed_back.empty()) {
+        Slot &sl = *sv->handed_back.front();
+        sv->handed_back.pop_front();
+        sv->reserved -= sl.reserved;
+        sl.reserved = 0;
+        sl.reqs.clear();
+        sl.kind = -1;
+        any = true;
+      }
+    }
     for (auto &sl : sv->slots) {
       if (sl.kind < 0) continue;
       cudaError_t e = cudaEventQuery(sl.done);
+      if (e == cudaSuccess) {
+        const Clock::time_point now = Clock::now();
+        for (Req *q : sl.reqs) q->t_device_done = now;
+        sl.launched = sl.kind;
+        sl.kind = -3;
+        {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          sv->to_complete.push_back(&sl);
+        }
+        sv->cv_complete.notify_one();
+        any = true;
+        continue;
+      }
       if (e == cudaErrorNotReady) {
         double waited = std::chrono::duration<double, std::milli>(Clock::now() - sl.t_launch).count();
         if (waited < (double)sv->cfg.device_wait_limit_ms) continue;
         for (Req *q : sl.reqs) finish(sv, q, HM_ETIMEOUT);
         sl.retired = true;
-      } else if (e != cudaSuccess) {
-        for (Req *q : sl.reqs) finish(sv, q, cuda_err(e));
       } else {
-        const Clock::time_point now = Clock::now();
-        for (Req *q : sl.reqs) q->t_device_done = now;
-        if (sl.kind == HM_REQ_SEARCH)
-          complete_points(sv, sl);
-        else
-          complete_ranges(sv, sl);
+        for (Req *q : sl.reqs) finish(sv, q, cuda_err(e));
       }
       {
         std::lock_guard<std::mutex> lk(sv->mu);
@@ -398,7 +432,39 @@ bool poll_slots(hm_server *sv, int64_t wait_us) {
   }
 }
 
+// The completer thread: copies finished launches' results to the callers'
+// buffers, finishes their requests, hands the slots back to the dispatcher.
+void completer(hm_server *sv) {
+  for (;;) {
+    Slot *sl = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      sv->cv_complete.wait(lk, [sv] { return sv->completer_quit || !sv->to_complete.empty(); });
+      if (sv->to_complete.empty()) return;  // quit, nothing left
+      sl = sv->to_complete.front();
+      sv->to_complete.pop_front();
+    }
+    if (sl->launched == HM_REQ_SEARCH)
+      complete_points(sv, *sl);
+    else
+      complete_ranges(sv, *sl);
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->handed_back.push_back(sl);
+    }
+    sv->cv_submit.notify_all();  // the dispatcher may be waiting for a free slot
+  }
+}
+
+// A launch is running on the device, or its results are being copied out.
 bool slots_busy(hm_server *sv) {
+  for (auto &sl : sv->slots)
+    if (sl.kind >= 0 || sl.kind == -3) return true;
+  return false;
+}
+
+// A launch is running on the device (what a write epoch must wait for).
+bool slots_in_flight(hm_server *sv) {
   for (auto &sl : sv->slots)
     if (sl.kind >= 0) return true;
   return false;
@@ -413,7 +479,10 @@ Slot *free_slot_of(hm_server *sv) {
 // Applies a run of upserts as one epoch after every earlier request finished.
 void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
   const Clock::time_point t0 = Clock::now();
-  while (slots_busy(sv)) poll_slots(sv, 1000);
+  // the device work of every earlier read must be done; their results may
+  // still be on the way to the callers (the completer copies them from
+  // pinned staging, which the epoch does not touch)
+  while (slots_in_flight(sv)) poll_slots(sv, 1000);
   const Clock::time_point t1 = Clock::now();
   hm_tree *t = sv->t;
   int64_t n = 0;
@@ -423,12 +492,11 @@ void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
   // rebuild that frees the old arrays) under them, so writes fail from then on.
   bool retired = false;
   for (auto &x : sv->slots) retired |= x.kind == -2;
-  Slot *fs = free_slot_of(sv);
-  if (!fs || retired) {
+  if (retired) {
     for (Req *q : ups) finish(sv, q, HM_ETIMEOUT);
     return;
   }
-  Slot &sl = *fs;
+  Slot &sl = sv->epoch_slot;
   const bool del = ups[0]->r.kind == HM_REQ_DELETE;
   const size_t b = align_up(std::max<int64_t>(n, 1) * 8, 256);
   int rc = slot_reserve(sl, 2 * b, 2 * b);
@@ -656,9 +724,31 @@ int hm_server_start(hm_tree *t, const hm_server_config *cfg, hm_server **out) {
       }
     }
   }
+  {
+    Slot &es = sv->epoch_slot;
+    cudaError_t e = cudaStreamCreateWithFlags(&es.s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&es.done, cudaEventDisableTiming);
+    if (e == cudaSuccess && slot_reserve(es, 2 << 20, 2 << 20) != HM_OK) e = cudaErrorMemoryAllocation;
+    if (e != cudaSuccess) {
+      if (es.dev) cudaFree(es.dev);
+      if (es.pin) cudaFreeHost(es.pin);
+      if (es.done) cudaEventDestroy(es.done);
+      for (auto &x : sv->slots) {
+        if (x.dev) cudaFree(x.dev);
+        if (x.pin) cudaFreeHost(x.pin);
+        if (x.s) cudaStreamDestroy(x.s);
+        if (x.done) cudaEventDestroy(x.done);
+      }
+      if (es.s) cudaStreamDestroy(es.s);
+      delete sv;
+      return cuda_err(e);
+    }
+  }
   sv->t_start = Clock::now();
   const unsigned hw = std::thread::hardware_concurrency();
-  sv->copies.start((int)std::min(8u, std::max(1u, hw / 3)));
+  sv->copies.start((int)std::min(8u, std::max(1u, hw / 4)));
+  sv->copies_out.start((int)std::min(8u, std::max(1u, hw / 4)));
+  sv->completer = std::thread(completer, sv);
   sv->th = std::thread(dispatcher, sv);
   *out = sv;
   return HM_OK;
@@ -778,8 +868,15 @@ int hm_server_stop(hm_server *sv) {
     sv->cv_submit.notify_all();
   }
   for (Req *q : cancelled) finish(sv, q, HM_ECANCELLED);
-  if (sv->th.joinable()) sv->th.join();
+  if (sv->th.joinable()) sv->th.join();  // returns once every launch is completed
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->completer_quit = true;
+  }
+  sv->cv_complete.notify_all();
+  if (sv->completer.joinable()) sv->completer.join();
   sv->copies.stop();
+  sv->copies_out.stop();
   return HM_OK;
 }
 
@@ -792,6 +889,13 @@ int hm_server_free(hm_server *sv) {
     if (sl.pin) cudaFreeHost(sl.pin);
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.s) cudaStreamDestroy(sl.s);
+  }
+  {
+    Slot &es = sv->epoch_slot;
+    if (es.dev) cudaFree(es.dev);
+    if (es.pin) cudaFreeHost(es.pin);
+    if (es.done) cudaEventDestroy(es.done);
+    if (es.s) cudaStreamDestroy(es.s);
   }
   for (auto &kv : sv->reqs) delete kv.second;
   delete sv;
