@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--leaf-cap", type=int, default=16)
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (use the flags below)")
     ap.add_argument("--group-width", type=int, default=4)
-    ap.add_argument("--qpg", type=int, default=2)
+    ap.add_argument("--qpg", type=int, default=1)
     ap.add_argument("--sort-bits", type=int, default=-1)
     ap.add_argument("--hints", type=int, default=1)
     ap.add_argument("--join", type=int, default=-1, help="1 bucket join, 2 never, -1 auto")
@@ -229,6 +229,7 @@ def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
 
     tree.search(q[: 1 << 20], threads)  # warm
     sec = median_s(lambda: tree.search(q, threads))
+    cpu_out = tree.search(q, threads)
     res = {"build_s": round(build_s, 1), "cores": threads,
            "search": {"value": round(m / sec / 1e6, 3), "unit": UNIT, "ms_per_step": round(sec * 1e3, 1),
                       "sample": f"the whole {m}-query batch, median of 3"}}
@@ -244,16 +245,12 @@ def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
                 g = po.RefGpuSearch(tree)
                 out, md, mc = g.search(q, reps=5)
                 g.close()
-                gold = _golden("c2_point")
-                if gold and gold["n"] == n and gold["m"] == m and gold["hit"] == hit:
-                    ok = _digest(out) == gold["digest"]
-                    check = "results equal the reference CPU tree's (golden c2_point digest)" if ok else "DIFFERS"
-                else:
-                    ok = bool((out[: 1 << 16] == tree.search(q[: 1 << 16], threads)).all())
-                    check = "results equal the reference CPU tree's on 2^16 queries" if ok else "DIFFERS"
+                wrong = int((out != cpu_out).sum())
+                check = (f"{wrong} of {m} results differ from the reference's own CPU search "
+                         f"({int(((out == -1) & (cpu_out >= 0)).sum())} hits returned as misses)")
                 res["gpu"] = {"value": round(m / md / 1e3, 1), "unit": UNIT, "ms_per_step": round(md, 4),
                               "with_copies": {"value": round(m / mc / 1e3, 1), "unit": UNIT, "ms_per_step": round(mc, 3)},
-                              "check": check,
+                              "wrong_results": wrong, "check": check,
                               "what": "the reference's GPU search compiled for sm_100a (open-harmonia/src/full-multi-"
                                       "prefix-sort-8thread.cu: CUB SortPairs on bits [48,64) + the 8-thread kernel) "
                                       "on its own PPI tree, device-resident keys, mean of 5; with_copies adds the "
@@ -392,7 +389,7 @@ def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
         for q, out in batches:
             tree.search(q, out)
 
-    tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0, join=2)
+    tree.set_search_config(group_width=4, queries_per_group=1, sort_bits=0, join=2)
     for _ in range(warmup):
         per_batch()
     plain_ms = timed(steps, per_batch)
@@ -423,7 +420,7 @@ def batched_uneven(tree, keys, sk, dev, timed, steps, warmup, seed=7):
             "check": check,
             "plain_per_batch": {"value": round(total / plain_ms / 1e3, 1), "unit": UNIT,
                                 "ms_per_step": round(plain_ms, 3),
-                                "what": "one search launch per batch, unsorted, group width 4, 2 queries/group"},
+                                "what": "one search launch per batch, unsorted, group width 4, 1 query per group (the default)"},
             "tuned_per_batch": {"value": round(total / tuned_ms / 1e3, 1), "unit": UNIT,
                                 "ms_per_step": round(tuned_ms, 3),
                                 "what": "hm_search with the tuned configuration once per batch (pre-sort and "
@@ -514,8 +511,8 @@ def fanout_128(keys, q, d_q, dev, timed, steps, warmup, exp):
             r["algorithmic_gbs"] = round(bq * m / (ms * 1e-3) / 1e9, 1)
         res[name] = r
 
-    t.set_search_config(group_width=4, queries_per_group=2, sort_bits=0, join=2)
-    run("plain", d_q, "one descent launch on the unsorted batch, group width 4, 2 queries per group", 240)
+    t.set_search_config(group_width=4, queries_per_group=1, sort_bits=0, join=2)
+    run("plain", d_q, "one descent launch on the unsorted batch, group width 4, 1 query per group (the default)", 240)
     assert (out[:4096].cpu().numpy() == exp).all(), "fanout-128 results are wrong"
     order = np.argsort(q >> np.int64(47), kind="stable")
     d_qs = torch.from_numpy(q[order]).to(dev)
@@ -721,13 +718,13 @@ def main():
     extras = {}
     # plain single-batch launch: unsorted, default group width/depth, no tuning
     if args.extras:
-        tree.set_search_config(group_width=4, queries_per_group=2, sort_bits=0, join=2)
+        tree.set_search_config(group_width=4, queries_per_group=1, sort_bits=0, join=2)
         for _ in range(args.warmup):
             tree.search(d_q, d_out)
         plain_ms = timed(args.steps, lambda: tree.search(d_q, d_out))
         extras["plain"] = {"value": round(ws * m / plain_ms / 1e3, 1), "unit": UNIT, "ms_per_step": round(plain_ms, 4),
                            "what": "one launch of the search kernel on the unsorted batch, group width 4, "
-                                   "2 queries per group, no pre-sort"}
+                                   "1 query per group (the default configuration), no pre-sort"}
     tree.set_search_config(group_width=args.group_width, queries_per_group=args.qpg,
                            sort_bits=args.sort_bits, cache_hints=args.hints, join=args.join)
     tuned = tree.config()

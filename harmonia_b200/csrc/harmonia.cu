@@ -241,7 +241,7 @@ void fill_defaults(hm_config *c) {
   if (c->inner_fill == 0) c->inner_fill = c->fanout;
   if (c->leaf_fill == 0) c->leaf_fill = c->leaf_cap;
   if (c->group_width == 0) c->group_width = 4;
-  if (c->queries_per_group == 0) c->queries_per_group = 2;
+  if (c->queries_per_group == 0) c->queries_per_group = 1;
   if (c->smem_bytes == 0) c->smem_bytes = 48 * 1024;
   if (c->cache_hints == 0) c->cache_hints = 1;
   if (c->join == 0) c->join = -1;

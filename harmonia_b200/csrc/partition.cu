@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_ke
 // chunk's result copies are in flight, which takes two dependent round trips
 // off every chunk but the first.  The per-chunk work is the same as above.
 #ifndef HM_PSA_REV_PERSIST
-#define HM_PSA_REV_PERSIST 0
+#define HM_PSA_REV_PERSIST 1  // measured: both inverse passes 0.178 -> 0.169 ms at 2^24 queries
 #endif
 template <bool BATCHED>
 __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_persist_kernel(

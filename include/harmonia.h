@@ -80,7 +80,8 @@ typedef struct {
   int inner_fill;        /* children per inner node at bulk load, 2..fanout (default fanout) */
   int leaf_fill;         /* keys per leaf at bulk load, 1..leaf_cap (default leaf_cap) */
   int group_width;       /* lanes cooperating on one query: 1,2,4,8,16,32 (default 4) */
-  int queries_per_group; /* queries a group keeps in flight: 1,2,4 (default 2) */
+  int queries_per_group; /* queries a group keeps in flight: 1,2,4 (default 1; at 1 a 16-key leaf's
+                            values load with its keys) */
   int sort_bits;         /* query pre-sort: top bits, 0 = off, 1..16, -1 = auto (default -1) */
   int smem_bytes;        /* budget for top levels staged in shared memory (default 49152) */
   int cache_hints;       /* L2 policy: 1 = inner rows evict_last, leaves evict_first; 2 = none

@@ -248,6 +248,7 @@ def _ref_lib(path: str = REF_SO):
             lib.hmrefgpu_search.argtypes = [_P, _P, _L, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                                             ctypes.POINTER(ctypes.c_float)]
             lib.hmrefgpu_search.restype = ctypes.c_int
+            lib.hmrefgpu_emulate.argtypes = [_P, _P, _L, _P]
         _ref[path] = lib
     return _ref[path]
 
@@ -409,4 +410,13 @@ def check_gpu_ref_batch(tree: RefTree, q) -> int:
     """The CPU check of the reference GPU kernel's index path alone."""
     q = np.ascontiguousarray(q, dtype=np.int64)
     return int(_ref_lib(GPU_SO).hmrefgpu_check(tree.h, _ptr(q), len(q)))
+
+
+def emulate_gpu_ref(tree: RefTree, q) -> np.ndarray:
+    """The reference GPU kernel's computation run on the CPU (for locating
+    where its results depart from the CPU search); -7 marks refused keys."""
+    q = np.ascontiguousarray(q, dtype=np.int64)
+    out = np.empty_like(q)
+    _ref_lib(GPU_SO).hmrefgpu_emulate(tree.h, _ptr(q), len(q), _ptr(out))
+    return out
 

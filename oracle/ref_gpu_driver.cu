@@ -154,6 +154,59 @@ long hmrefgpu_check(void *hp, const long long *q, long n) {
   return bad;
 }
 
+// The kernel's whole per-key computation on the CPU (descent as check_one,
+// then the leaf phase of :214-252: the first of the record list's 4 slots
+// whose key is >= the query, a hit if equal), decoded as the driver decodes
+// the GPU's results; out[i] = the value or -1, or -7 for a key the check
+// refuses.  For finding where the GPU results depart from the CPU search.
+void hmrefgpu_emulate(void *hp, const long long *q, long n, long long *out) {
+  BPlusTree *t = static_cast<BPlusTree *>(hmref_ppi_tree(hp));
+  RefGpu g;
+  g.t = t;
+  g.n_inner = t->getInnerSize();
+  g.n_bleaf = t->getBLeafSize();
+  g.root = t->getRootIdx();
+  g.height = t->getHeight();
+  g.inner_wo_last = t->getInnerSize_wo_last_inner_node();
+  const int *prefix = t->getPrefixArray();
+  for (long i = 0; i < n; i++) {
+    const key_t target = q[i];
+    if (target == Max_Key || !check_one(g, prefix, target)) {
+      out[i] = -7;
+      continue;
+    }
+    int pos = g.root, relist = 0;
+    for (int lv = 1; lv < g.height; lv++) {
+      const Inner_node *node = t->getInnerNodeByIdx(pos);
+      int s = 0;
+      while (s < 8 && !(target < node->inner_index[s])) s++;
+      const int begin = s * 8;
+      int idx = begin + 8;
+      for (int k = 0; k < 8; k++)
+        if (target < node->inner_key[begin + k]) {
+          idx = begin + k;
+          break;
+        }
+      if (lv == g.height - 1) {
+        pos -= g.inner_wo_last;
+        relist = idx;
+      } else {
+        pos = prefix[pos] + idx;
+      }
+    }
+    const BLeaf_node *leaf = t->getBLeafNodeByIdx(pos);
+    long long v = -1;
+    for (int s2 = 0; s2 < 4; s2++) {
+      const key_t k = leaf->relist[relist].r[s2].r_key;
+      if (target <= k) {
+        if (k == target) v = leaf->relist[relist].r[s2].val;
+        break;
+      }
+    }
+    out[i] = v;
+  }
+}
+
 void hmrefgpu_free(void *h) {
   if (h) release(static_cast<RefGpu *>(h));
 }

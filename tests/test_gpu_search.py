@@ -81,7 +81,7 @@ def test_every_group_width_and_depth(c1, w, qpg):
     try:
         assert (t.search(cuda(q)).cpu().numpy() == exp).all()
     finally:
-        t.set_search_config(group_width=4, queries_per_group=2, sort_bits=-1, join=-1)
+        t.set_search_config(group_width=4, queries_per_group=1, sort_bits=-1, join=-1)
 
 
 @pytest.mark.parametrize("bits", [1, 4, 8, 9, 12, 16])
@@ -175,7 +175,7 @@ def test_autotune_keeps_results_exact(c1):
     assert best["join"] in (-1, 2)  # the join is left to the automatic choice or switched off
     exp = po.PortTree(sk, dg.values_for(sk)).search(q)
     assert (t.search(cuda(q)).cpu().numpy() == exp).all()
-    t.set_search_config(group_width=4, queries_per_group=2, sort_bits=-1, join=-1)
+    t.set_search_config(group_width=4, queries_per_group=1, sort_bits=-1, join=-1)
 
 
 def test_launches_come_from_the_library(c1):
