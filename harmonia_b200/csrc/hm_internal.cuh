@@ -164,8 +164,9 @@ struct hm_tree {
   // (ScratchLease).  A block is ordered on the device after its previous use
   // by the event recorded at the end of that use, so reads enqueued on
   // different streams (or from different host threads) never share a block
-  // while either runs, and a block grows with a stream-ordered free and
-  // allocation instead of a device-wide synchronisation.
+  // while either runs.  A block that is too small is replaced by one half
+  // again as large and retired (freed with the tree, never during a call:
+  // cudaFree synchronises the device).
   struct ScratchBlock {
     void *ptr = nullptr;
     size_t bytes = 0;
@@ -177,6 +178,7 @@ struct hm_tree {
   };
   std::vector<ScratchBlock> pool;
   uint64_t pool_tick = 0;
+  std::vector<void *> retired;  // outgrown blocks, freed with the tree
   // guards the host-side state that concurrent calls share: the scratch pool,
   // the join boundary cache, the comparison kernel's child ids and the
   // profiling records
@@ -321,6 +323,17 @@ struct BatchView {
   int nb = 0;
 };
 
+// Pre-sort for a consumer that places its results itself (bits in 9..16):
+// the first pass as partition_queries (offset mode), the second records in
+// place[i] the position grouped query i had after the first pass.  Results
+// written to res1[place[i]] are in first-pass order, which
+// unpermute_first_pass takes back to the input order.
+int partition_queries_placed(const hm_tree *t, const int64_t *q, int64_t n, int bits, int64_t *q_out,
+                             int32_t *place, void *scratch, cudaStream_t s, const int64_t **bucket_start,
+                             const BatchView *bv = nullptr);
+int unpermute_first_pass(int64_t n, int bits, const int64_t *res1, int64_t *out, void *scratch, cudaStream_t s,
+                         const BatchView *bv = nullptr);
+
 // offsets: the partition keeps chunk offsets in the scratch for
 // unpermute_results (pos_out == nullptr); else it writes input positions.
 size_t partition_scratch_bytes(int64_t n, int bits, bool offsets, int batches = 1);  // batches: of a batch set
@@ -370,8 +383,10 @@ void prof_end(hm_tree *t, int stage, int token, cudaStream_t s);
 int join_bits(const hm_tree *t);   // bucket bits for the join (leaves per bucket fit shared memory)
 bool join_fits(const hm_tree *t);  // the join supports this leaf size and its buckets fit on average
 size_t join_scratch_bytes(int64_t n, int bits);
-int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int bits,
-                int64_t n, int64_t *out, void *scratch, cudaStream_t s);
+// place: nullptr = results in grouped order (out[i] for grouped query i);
+// else out[place[i]].
+int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int bits, int64_t n, int64_t *out,
+                void *scratch, cudaStream_t s, const int32_t *place = nullptr);
 
 // Opts kernel fn in to `bytes` of dynamic shared memory (and the largest
 // shared-memory carveout) on the current device; once per device, kernel and
@@ -385,6 +400,7 @@ int opt_in_smem(const void *fn, int bytes);
 struct SearchPlan {
   int bits = 0;
   bool join = false;
+  bool placed = false;  // the join writes its results in first-pass order (two-pass pre-sort)
   int batches = 1;  // batches of a batch set (its first pre-sort pass cuts each batch apart)
   size_t scratch = 0;
 };
@@ -405,7 +421,7 @@ void refresh_smem_levels(hm_tree *t);
 // stream s.  acquire(bytes) picks an idle block (the one last used on s, else
 // one whose last use has finished, else a new one while the pool is small,
 // else the one idle longest), makes s wait for the block's previous use and
-// grows it on s if needed.  The destructor records the end of this use on s
+// replaces it by a larger one if needed.  The destructor records the end of this use on s
 // and returns the block to the pool, so the caller must have enqueued all
 // work that touches the block by then.  A stream under graph capture gets
 // HM_EINVAL: captured work uses memory the graph owns (hm_plan_create).

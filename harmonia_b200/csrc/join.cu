@@ -53,8 +53,14 @@ static_assert(kItemMax < 65536, "an item's query count is kept in 16 bits");
 constexpr int kStages = HM_JOIN_STAGES;
 constexpr int kStageMax = (216 / kStages) * 1024;  // shared memory of one stage, at most
 
-// A work item: at most kItemMax queries of one bucket and the bucket's leaves
-// [l0, l0 + nl); the leaves are staged once for all of them.
+#ifndef HM_JOIN_MAX_BITS
+#define HM_JOIN_MAX_BITS 16
+#endif
+static_assert(HM_JOIN_MAX_BITS <= 16, "a bucket number is kept in 16 bits");
+
+// A work item: at most kItemMax queries of one bucket, grouped queries
+// [qa, qa + len), and the bucket's leaves [l0, l0 + nl); the leaves are
+// staged once for all of them.
 struct __align__(16) Item {
   int32_t qa, l0, b;  // first query, first leaf, bucket
   uint32_t len_nl;    // queries (at most kItemMax) << 16 | leaves (capped at 65535)
@@ -72,7 +78,7 @@ __global__ void bucket_prep_kernel(DevTree t, int f, int64_t lo, int shift, int 
                                    int32_t *__restrict__ cnt, bool want_leafb) {
   pdl_enter();
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x) {
-    cnt[b] = b < nb ? (int32_t)((bstart[b + 1] - bstart[b] + kItemMax - 1) / kItemMax) : 0;
+    if (cnt) cnt[b] = b < nb ? (int32_t)((bstart[b + 1] - bstart[b] + kItemMax - 1) / kItemMax) : 0;
     if (!want_leafb) continue;
     if (b == 0) {
       leafb[0] = 0;
@@ -257,13 +263,15 @@ __device__ __noinline__ int64_t lookup_scalar(const DevTree &t, int f, int64_t q
 // in flight (cp.async) while the current one is answered from shared memory,
 // kRun queries per step.  Item descriptors are loaded kStages items ahead and
 // the queries of the next step (of this item or the next) one step ahead.
-// Results are written in the grouped order (out[i] for grouped query i).
 // DIR: each staged item first builds its directory (batches with many queries
 // per bucket); otherwise a query binary-searches the staged first keys.
-template <int LC, bool DIR>
+// PLACED: grouped query i's result goes to out[place[i]] (its position before
+// the last pre-sort pass, which the pass recorded), else to out[i].
+template <int LC, bool DIR, bool PLACED>
 __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t, int f, const Item *__restrict__ items,
                                                         const int64_t *__restrict__ nitems,
-                                                        const int64_t *__restrict__ qs, int64_t *__restrict__ out,
+                                                        const int64_t *__restrict__ qs,
+                                                        const int32_t *__restrict__ place, int64_t *__restrict__ out,
                                                         int ml, uint64_t key_lo_u, int shift) {
   pdl_enter();
   static_assert(kStages >= 2, "a ring of at least two stages");
@@ -285,10 +293,13 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
     cp_async_commit();
   }
   int64_t q[kPerThread];
+  int32_t qo[kPerThread];  // where each result goes
 #pragma unroll
   for (int j = 0; j < kPerThread; j++) {
     const int r = j * kThreads + threadIdx.x;
-    q[j] = r < d[0].len() ? __ldg(qs + d[0].qa + r) : 0;
+    const bool in = r < d[0].len();
+    q[j] = in ? __ldg(qs + d[0].qa + r) : 0;
+    qo[j] = PLACED ? (in ? __ldg(place + d[0].qa + r) : 0) : d[0].qa + r;
   }
   int cur_stage = 0;
   for (; it < n_items; it += g) {
@@ -314,10 +325,13 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
       const int32_t na = more ? cur.qa + r0 + kRun : d[1].qa;
       const int32_t nlen = more ? cur.len() - r0 - kRun : d[1].len();
       int64_t qn[kPerThread];
+      int32_t on[kPerThread];
 #pragma unroll
       for (int j = 0; j < kPerThread; j++) {
         const int r = j * kThreads + threadIdx.x;
-        qn[j] = r < nlen ? __ldg(qs + na + r) : 0;
+        const bool in = r < nlen;
+        qn[j] = in ? __ldg(qs + na + r) : 0;
+        on[j] = PLACED ? (in ? __ldg(place + na + r) : 0) : na + r;
       }
 #pragma unroll
       for (int j = 0; j < kPerThread; j++) {
@@ -332,10 +346,13 @@ __global__ void __launch_bounds__(kThreads, HM_JOIN_MINB) join_kernel(DevTree t,
           else
             v = lookup_staged<LC>(st, cur.nl(), span, q[j]);
         }
-        out[cur.qa + r] = v;  // grouped order: consecutive threads, consecutive slots
+        out[qo[j]] = v;  // grouped order: consecutive threads, consecutive slots
       }
 #pragma unroll
-      for (int j = 0; j < kPerThread; j++) q[j] = qn[j];
+      for (int j = 0; j < kPerThread; j++) {
+        q[j] = qn[j];
+        qo[j] = on[j];
+      }
     }
     __syncthreads();  // this stage is refilled in the next iteration
 #pragma unroll
@@ -362,9 +379,6 @@ int stage_leaves_for(const hm_tree *t, int bits) {
 
 }  // namespace
 
-#ifndef HM_JOIN_MAX_BITS
-#define HM_JOIN_MAX_BITS 16
-#endif
 int join_bits(const hm_tree *t) {
   // HM_JOIN_MAX_BITS bits, or fewer while buckets still average at most 32 leaves
   int b = 1;
@@ -387,28 +401,27 @@ size_t join_scratch_bytes(int64_t n, int bits) {
          256;
 }
 
-int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int bits,
-                int64_t n, int64_t *out, void *scratch, cudaStream_t s) {
-  if (n <= 0) return HM_OK;
-  const int nb = 1 << bits;
-  char *p = static_cast<char *>(scratch);
-  int32_t *leafb = reinterpret_cast<int32_t *>(p);
-  p += align_up(4 * (nb + 1), 256);
-  int32_t *cnt = reinterpret_cast<int32_t *>(p);
-  p += align_up(4 * (nb + 1), 256);
-  int64_t *first = reinterpret_cast<int64_t *>(p);
-  p += align_up(8 * (nb + 2), 256);
-  void *scan = p;
-  p += align_up((int64_t)scan_scratch_bytes(nb + 1), 256);  // keeps the 16-B items aligned
-  Item *items = reinterpret_cast<Item *>(p);
-  // bucket geometry, as the partition computed it
+namespace {
+
+// Bucket geometry, as the partition computes it: bucket of k = (k - key_min) >> shift.
+int bucket_shift(const hm_tree *t, int bits) {
   uint64_t range = (uint64_t)t->key_max - (uint64_t)t->key_min;
   int len = 0;
   while (len < 64 && (range >> len) != 0) len++;
-  const int shift = len > bits ? len - bits : 0;
+  return len > bits ? len - bits : 0;
+}
+
+// The leaf of each bucket boundary (nb + 1 entries): kept per tree shape in
+// the tree, else computed into leafb_scratch.  With bstart (contiguous
+// buckets) the same launch writes each bucket's item count into cnt; without
+// it the launch is skipped when the kept boundaries are valid.
+const int32_t *bucket_bounds(const hm_tree *t, int bits, int shift, const int64_t *bstart, int32_t *leafb_scratch,
+                             int32_t *cnt, cudaStream_t s) {
+  const int nb = 1 << bits;
   const unsigned gb = (unsigned)((nb + 1 + 255) / 256);
-  // the boundaries' leaves: kept per tree shape (not inside a graph capture,
-  // whose replays must follow later changes of the tree)
+  int32_t *leafb = leafb_scratch;
+  // kept per tree shape (not inside a graph capture, whose replays must
+  // follow later changes of the tree)
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
     cudaGetLastError();
@@ -449,8 +462,11 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
       }
     }
   }
-  launch_pdl(bucket_prep_kernel, gb, 256, 0, s, t->view(), t->cfg.fanout, t->key_min, shift, nb, bstart, leafb, cnt,
-             want_leafb);
+  if (want_leafb || bstart) {
+    launch_pdl(bucket_prep_kernel, gb, 256, 0, s, t->view(), t->cfg.fanout, t->key_min, shift, nb, bstart, leafb,
+               bstart ? cnt : nullptr, want_leafb);
+    note_launch();
+  }
   if (fill_cache && cudaEventRecord(t->join_leafb_ready, s) == cudaSuccess) {
     t->join_leafb_valid = true;
     t->join_leafb_gen = t->generation;
@@ -460,26 +476,65 @@ int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int 
     t->join_leafb_nleaf = t->n_leaf;
     t->join_leafb_bits = bits;
   }
-  if (cache_lock.owns_lock()) cache_lock.unlock();
-  exclusive_scan_i32(cnt, first, nb + 1, scan, s);
-  launch_pdl(expand_items_kernel, gb, 256, 0, s, nb, bstart, leafb, cnt, first, items);
+  return leafb;
+}
+
+using JoinKernel = void (*)(DevTree, int, const Item *, const int64_t *, const int64_t *, const int32_t *, int64_t *,
+                            int, uint64_t, int);
+
+template <bool PLACED>
+JoinKernel pick_join(int lc, bool dir) {
+  if (lc == 16) return dir ? join_kernel<16, true, PLACED> : join_kernel<16, false, PLACED>;
+  if (lc == 64) return dir ? join_kernel<64, true, PLACED> : join_kernel<64, false, PLACED>;
+  return nullptr;
+}
+
+// Launches the join over the items (their count at nitems).
+int run_join(const hm_tree *t, JoinKernel k, int bits, int64_t n_items_max, const Item *items, const int64_t *nitems,
+             const int64_t *qs, const int32_t *place, int64_t *out, int shift, cudaStream_t s) {
+  if (!k) return HM_EINVAL;
   const int lc = t->cfg.leaf_cap;
   const int ml = stage_leaves_for(t, bits);
   const size_t smem = (size_t)kStages * ml * leaf_bytes(lc);
   const int per_sm = std::max(1, std::min(8, (int)((227 * 1024) / (smem + 1024))));
-  const unsigned grid = (unsigned)std::min<int64_t>(max_items(n, nb), (int64_t)t->num_sms * per_sm);
-  // measured: the directory pays from about three queries per thread and item
-  const bool dir = HM_JOIN_DIR_BITS > 0 && n >= (int64_t)HM_JOIN_DIR_MIN * nb;
-  using Kernel = void (*)(DevTree, int, const Item *, const int64_t *, const int64_t *, int64_t *, int, uint64_t, int);
-  Kernel k = nullptr;
-  if (lc == 16) k = dir ? join_kernel<16, true> : join_kernel<16, false>;
-  else if (lc == 64) k = dir ? join_kernel<64, true> : join_kernel<64, false>;
-  else return HM_EINVAL;
+  const unsigned grid = (unsigned)std::min<int64_t>(n_items_max, (int64_t)t->num_sms * per_sm);
   int rc = opt_in_smem((const void *)k, kStages * kStageMax);
   if (rc) return rc;
-  launch_pdl(k, grid, kThreads, smem, s, t->view(), t->cfg.fanout, items, first + nb, qs, out, ml, biased(t->key_min),
-             shift);
-  note_launch(3);
+  launch_pdl(k, grid, kThreads, smem, s, t->view(), t->cfg.fanout, items, nitems, qs, place, out, ml,
+             biased(t->key_min), shift);
+  note_launch();
+  return HM_OK;
+}
+
+// measured: the directory pays from about three queries per thread and item
+bool use_dir(int64_t n, int nb) { return HM_JOIN_DIR_BITS > 0 && n >= (int64_t)HM_JOIN_DIR_MIN * nb; }
+
+}  // namespace
+
+int launch_join(const hm_tree *t, const int64_t *qs, const int64_t *bstart, int bits, int64_t n, int64_t *out,
+                void *scratch, cudaStream_t s, const int32_t *place) {
+  if (n <= 0) return HM_OK;
+  const int nb = 1 << bits;
+  char *p = static_cast<char *>(scratch);
+  int32_t *leafb_s = reinterpret_cast<int32_t *>(p);
+  p += align_up(4 * (nb + 1), 256);
+  int32_t *cnt = reinterpret_cast<int32_t *>(p);
+  p += align_up(4 * (nb + 1), 256);
+  int64_t *first = reinterpret_cast<int64_t *>(p);
+  p += align_up(8 * (nb + 2), 256);
+  void *scan = p;
+  p += align_up((int64_t)scan_scratch_bytes(nb + 1), 256);  // keeps the 16-B items aligned
+  Item *items = reinterpret_cast<Item *>(p);
+  const int shift = bucket_shift(t, bits);
+  const unsigned gb = (unsigned)((nb + 1 + 255) / 256);
+  const int32_t *leafb = bucket_bounds(t, bits, shift, bstart, leafb_s, cnt, s);
+  exclusive_scan_i32(cnt, first, nb + 1, scan, s);
+  launch_pdl(expand_items_kernel, gb, 256, 0, s, nb, bstart, leafb, cnt, first, items);
+  note_launch();
+  const JoinKernel k = place ? pick_join<true>(t->cfg.leaf_cap, use_dir(n, nb))
+                             : pick_join<false>(t->cfg.leaf_cap, use_dir(n, nb));
+  int rc = run_join(t, k, bits, max_items(n, nb), items, first + nb, qs, place, out, shift, s);
+  if (rc) return rc;
   return cuda_err(cudaGetLastError());
 }
 

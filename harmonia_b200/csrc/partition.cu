@@ -894,6 +894,43 @@ int partition_queries(const hm_tree *t, const int64_t *q, int64_t n, int bits, i
   return cuda_err(cudaGetLastError());
 }
 
+int partition_queries_placed(const hm_tree *t, const int64_t *q, int64_t n, int bits, int64_t *q_out,
+                             int32_t *place, void *scratch, cudaStream_t s, const int64_t **bucket_start,
+                             const BatchView *bv) {
+  if (n == 0) return HM_OK;
+  if (bits <= 8 || bits > 16 || n > INT32_MAX || n < 0 || !place) return HM_EINVAL;
+  Work w;
+  work_layout(n, bits, true, &w, static_cast<char *>(scratch), bv ? bv->nb : 1);
+  const Bucket bk = make_bucket(t, bits);
+  const int sms = t->num_sms;
+  const int low = bits - 8;
+  uint16_t *loc1 = static_cast<uint16_t *>(w.pay1);
+  if (bv)
+    one_pass<uint16_t, false, true>(bk, nullptr, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1, w.p1,
+                                    w.scan, sms, s, *bv, w.cio);
+  else
+    one_pass<uint16_t, false>(bk, q, nullptr, n, nullptr, 1, low, 0xff, w.q_tmp, loc1, w.bstart1, w.p1, w.scan, sms,
+                              s);
+  one_pass<int32_t, false>(bk, w.q_tmp, nullptr, n, w.bstart1, 256, 0, (1 << low) - 1, q_out, place, w.bstart, w.p2,
+                           w.scan, sms, s);
+  if (bucket_start) *bucket_start = w.bstart;
+  return cuda_err(cudaGetLastError());
+}
+
+int unpermute_first_pass(int64_t n, int bits, const int64_t *res1, int64_t *out, void *scratch, cudaStream_t s,
+                         const BatchView *bv) {
+  if (n == 0) return HM_OK;
+  if (bits <= 8 || bits > 16 || n > INT32_MAX || n < 0) return HM_EINVAL;
+  Work w;
+  work_layout(n, bits, true, &w, static_cast<char *>(scratch), bv ? bv->nb : 1);
+  const uint16_t *loc1 = static_cast<const uint16_t *>(w.pay1);
+  if (bv)
+    unpermute_pass<true>(w.p1, 256, res1, loc1, nullptr, s, *bv, w.cio);
+  else
+    unpermute_pass(w.p1, 256, res1, loc1, out, s);
+  return cuda_err(cudaGetLastError());
+}
+
 int unpermute_results(int64_t n, int bits, int64_t *res_sorted, int64_t *out, void *scratch, cudaStream_t s,
                       const BatchView *bv) {
   if (n == 0) return HM_OK;

@@ -49,11 +49,15 @@ struct Req {
   Clock::time_point t_admit, t_enqueued, t_device_done;
   double latency_us = 0;
   size_t bytes = 0;  // device bytes the request needs while in flight
+  // point searches: keys / out are page-locked host or device memory, which
+  // the copy engines reach directly (no staging copy on the host)
+  bool direct_in = false, direct_out = false;
 };
 
 struct Slot {
   cudaStream_t s = nullptr;
-  cudaEvent_t done = nullptr;
+  cudaEvent_t done = nullptr;   // the launch's last copy finished
+  cudaEvent_t kdone = nullptr;  // its kernels (the last reads of the tree) finished
   char *dev = nullptr;
   size_t dev_bytes = 0;
   char *pin = nullptr;
@@ -151,6 +155,17 @@ class CopyPool {
   bool quit_ = false;
   std::vector<std::thread> th_;
 };
+
+// Page-locked host memory (cudaHostAlloc, cudaHostRegister) or device
+// memory: a copy engine reads or writes it without a staging copy.
+bool dma_reachable(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeDevice;
+}
 
 size_t req_device_bytes(const hm_request &r) {
   switch (r.kind) {
@@ -252,6 +267,16 @@ int slot_reserve(Slot &sl, size_t dev_need, size_t pin_need) {
   return HM_OK;
 }
 
+// Frees a slot's buffers, events and stream.
+void release_slot(Slot &x) {
+  if (x.dev) cudaFree(x.dev);
+  if (x.pin) cudaFreeHost(x.pin);
+  if (x.done) cudaEventDestroy(x.done);
+  if (x.kdone) cudaEventDestroy(x.kdone);
+  if (x.s) cudaStreamDestroy(x.s);
+  x = Slot();
+}
+
 // Enqueues a coalesced point search of sl.reqs on the slot's stream.
 int launch_points(hm_server *sv, Slot &sl) {
   hm_tree *t = sv->t;
@@ -262,20 +287,48 @@ int launch_points(hm_server *sv, Slot &sl) {
   int rc = slot_reserve(sl, 2 * qb + scr + 256, 2 * qb);
   if (rc) return rc;
   int64_t *hq = reinterpret_cast<int64_t *>(sl.pin);
+  int64_t *hout = reinterpret_cast<int64_t *>(sl.pin + qb);
   int64_t o = 0;
   std::vector<CopyJob> jobs;
   for (Req *q : sl.reqs) {
-    jobs.push_back({reinterpret_cast<char *>(hq + o), reinterpret_cast<const char *>(q->r.keys), q->r.n * 8});
+    if (!q->direct_in)
+      jobs.push_back({reinterpret_cast<char *>(hq + o), reinterpret_cast<const char *>(q->r.keys), q->r.n * 8});
     o += (int64_t)q->r.n;
   }
   sv->copies.run(jobs);
   int64_t *dq = reinterpret_cast<int64_t *>(sl.dev);
   int64_t *dout = reinterpret_cast<int64_t *>(sl.dev + qb);
-  cudaError_t e = cudaMemcpyAsync(dq, hq, n * 8, cudaMemcpyHostToDevice, sl.s);
+  // Inputs: staged requests in one copy per consecutive run, the others from
+  // their own buffers; results the same way back.
+  cudaError_t e = cudaSuccess;
+  auto copy_runs = [&](bool in) {
+    int64_t at = 0, run0 = -1;
+    auto flush = [&](int64_t end) {
+      if (run0 >= 0 && e == cudaSuccess)
+        e = in ? cudaMemcpyAsync(dq + run0, hq + run0, (end - run0) * 8, cudaMemcpyHostToDevice, sl.s)
+               : cudaMemcpyAsync(hout + run0, dout + run0, (end - run0) * 8, cudaMemcpyDeviceToHost, sl.s);
+      run0 = -1;
+    };
+    for (Req *q : sl.reqs) {
+      if (in ? q->direct_in : q->direct_out) {
+        flush(at);
+        if (e == cudaSuccess)
+          e = in ? cudaMemcpyAsync(dq + at, q->r.keys, q->r.n * 8, cudaMemcpyDefault, sl.s)
+                 : cudaMemcpyAsync(q->r.out, dout + at, q->r.n * 8, cudaMemcpyDefault, sl.s);
+      } else if (run0 < 0) {
+        run0 = at;
+      }
+      at += (int64_t)q->r.n;
+    }
+    flush(at);
+  };
+  copy_runs(true);
   if (e != cudaSuccess) return cuda_err(e);
   rc = run_search(t, dq, n, dout, sl.s, sl.dev + 2 * qb, scr);
   if (rc) return rc;
-  e = cudaMemcpyAsync(sl.pin + qb, dout, n * 8, cudaMemcpyDeviceToHost, sl.s);
+  e = cudaEventRecord(sl.kdone, sl.s);
+  if (e != cudaSuccess) return cuda_err(e);
+  copy_runs(false);
   if (e == cudaSuccess) e = cudaEventRecord(sl.done, sl.s);
   sl.n = n;
   return cuda_err(e);
@@ -287,7 +340,8 @@ void complete_points(hm_server *sv, Slot &sl) {
   int64_t o = 0;
   std::vector<CopyJob> jobs;
   for (Req *q : sl.reqs) {
-    jobs.push_back({reinterpret_cast<char *>(q->r.out), reinterpret_cast<const char *>(hout + o), q->r.n * 8});
+    if (!q->direct_out)
+      jobs.push_back({reinterpret_cast<char *>(q->r.out), reinterpret_cast<const char *>(hout + o), q->r.n * 8});
     o += (int64_t)q->r.n;
   }
   sv->copies_out.run(jobs);
@@ -335,6 +389,8 @@ int launch_ranges(hm_server *sv, Slot &sl) {
   exclusive_scan_i64(cnt, off, n, scan, sl.s);
   rc = range_copy_out(t, fl, fs, off, n, ok, ov, sl.s);
   if (rc) return rc;
+  e = cudaEventRecord(sl.kdone, sl.s);
+  if (e != cudaSuccess) return cuda_err(e);
   char *hoff = sl.pin + b8 + b4;
   e = cudaMemcpyAsync(hoff, off, (n + 1) * 8, cudaMemcpyDeviceToHost, sl.s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(hoff + b8, ok, recs * 8, cudaMemcpyDeviceToHost, sl.s);
@@ -479,10 +535,19 @@ Slot *free_slot_of(hm_server *sv) {
 // Applies a run of upserts as one epoch after every earlier request finished.
 void run_epoch(hm_server *sv, std::vector<Req *> &ups) {
   const Clock::time_point t0 = Clock::now();
-  // the device work of every earlier read must be done; their results may
-  // still be on the way to the callers (the completer copies them from
-  // pinned staging, which the epoch does not touch)
-  while (slots_in_flight(sv)) poll_slots(sv, 1000);
+  // Every earlier read's kernels must have ended before the epoch writes the
+  // tree; their result copies (device scratch to pinned staging) and the
+  // completer's copies out read no tree memory and may overlap the epoch.
+  // poll_slots retires a launch still unfinished after the device wait
+  // limit, which ends this wait too.
+  for (;;) {
+    bool reading = false;
+    for (auto &x : sv->slots)
+      if (x.kind >= 0 && cudaEventQuery(x.kdone) == cudaErrorNotReady) reading = true;
+    if (!reading) break;
+    poll_slots(sv, 200);
+  }
+  cudaGetLastError();  // a failed query is the launch's own error, reported by poll_slots
   const Clock::time_point t1 = Clock::now();
   hm_tree *t = sv->t;
   int64_t n = 0;
@@ -696,11 +761,9 @@ int hm_server_start(hm_tree *t, const hm_server_config *cfg, hm_server **out) {
   for (auto &sl : sv->slots) {
     cudaError_t e = cudaStreamCreateWithFlags(&sl.s, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.kdone, cudaEventDisableTiming);
     if (e != cudaSuccess) {
-      for (auto &x : sv->slots) {
-        if (x.s) cudaStreamDestroy(x.s);
-        if (x.done) cudaEventDestroy(x.done);
-      }
+      for (auto &x : sv->slots) release_slot(x);
       delete sv;
       return cuda_err(e);
     }
@@ -713,12 +776,7 @@ int hm_server_start(hm_tree *t, const hm_server_config *cfg, hm_server **out) {
     for (auto &sl : sv->slots) {
       int rc = slot_reserve(sl, dev, 2 * qb);
       if (rc) {
-        for (auto &x : sv->slots) {
-          if (x.dev) cudaFree(x.dev);
-          if (x.pin) cudaFreeHost(x.pin);
-          if (x.s) cudaStreamDestroy(x.s);
-          if (x.done) cudaEventDestroy(x.done);
-        }
+        for (auto &x : sv->slots) release_slot(x);
         delete sv;
         return rc;
       }
@@ -730,16 +788,8 @@ int hm_server_start(hm_tree *t, const hm_server_config *cfg, hm_server **out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&es.done, cudaEventDisableTiming);
     if (e == cudaSuccess && slot_reserve(es, 2 << 20, 2 << 20) != HM_OK) e = cudaErrorMemoryAllocation;
     if (e != cudaSuccess) {
-      if (es.dev) cudaFree(es.dev);
-      if (es.pin) cudaFreeHost(es.pin);
-      if (es.done) cudaEventDestroy(es.done);
-      for (auto &x : sv->slots) {
-        if (x.dev) cudaFree(x.dev);
-        if (x.pin) cudaFreeHost(x.pin);
-        if (x.s) cudaStreamDestroy(x.s);
-        if (x.done) cudaEventDestroy(x.done);
-      }
-      if (es.s) cudaStreamDestroy(es.s);
+      release_slot(es);
+      for (auto &x : sv->slots) release_slot(x);
       delete sv;
       return cuda_err(e);
     }
@@ -762,6 +812,10 @@ int hm_server_submit(hm_server *sv, const hm_request *r, uint64_t *ticket) {
   if (!q) return HM_ENOMEM;
   q->r = *r;
   q->bytes = req_device_bytes(*r);
+  if (r->kind == HM_REQ_SEARCH && r->n > 0) {
+    q->direct_in = dma_reachable(r->keys);
+    q->direct_out = dma_reachable(r->out);
+  }
   q->t_submit = Clock::now();
   std::lock_guard<std::mutex> lk(sv->mu);
   if (sv->stopping) {
@@ -883,20 +937,9 @@ int hm_server_stop(hm_server *sv) {
 int hm_server_free(hm_server *sv) {
   if (!sv) return HM_OK;
   hm_server_stop(sv);
-  for (auto &sl : sv->slots) {
-    if (sl.retired) continue;  // its stream may still own the buffers
-    if (sl.dev) cudaFree(sl.dev);
-    if (sl.pin) cudaFreeHost(sl.pin);
-    if (sl.done) cudaEventDestroy(sl.done);
-    if (sl.s) cudaStreamDestroy(sl.s);
-  }
-  {
-    Slot &es = sv->epoch_slot;
-    if (es.dev) cudaFree(es.dev);
-    if (es.pin) cudaFreeHost(es.pin);
-    if (es.done) cudaEventDestroy(es.done);
-    if (es.s) cudaStreamDestroy(es.s);
-  }
+  for (auto &sl : sv->slots)
+    if (!sl.retired) release_slot(sl);  // a retired slot's stream may still own its buffers
+  release_slot(sv->epoch_slot);
   for (auto &kv : sv->reqs) delete kv.second;
   delete sv;
   return HM_OK;

@@ -75,6 +75,10 @@ class Ticket:
         self.status = None
 
     def wait(self, timeout_us: int = -1, check_status: bool = True):
+        if self.status is not None:  # already collected
+            if check_status and self.status != 0:
+                raise HarmoniaError(self.status, "request")
+            return self._result()
         st = ctypes.c_int()
         rc = _bind().hm_server_wait(self.server._h, self.ticket, timeout_us, ctypes.byref(st))
         if rc != 0:
@@ -107,9 +111,15 @@ class Server:
             raise HarmoniaError(rc, "hm_server_submit")
         return t.value
 
-    def search(self, keys) -> Ticket:
+    def search(self, keys, out=None) -> Ticket:
+        """Point search; out (optional) receives the values.  keys and out in
+        page-locked memory (e.g. numpy views of torch tensors made with
+        pin_memory=True) are copied by DMA without a staging copy."""
         keys = np.ascontiguousarray(keys, dtype=np.int64)
-        out = np.empty(len(keys), np.int64)
+        if out is None:
+            out = np.empty(len(keys), np.int64)
+        elif out.dtype != np.int64 or not out.flags.c_contiguous or len(out) != len(keys):
+            raise ValueError("out must be a contiguous int64 array as long as keys")
         r = Request(kind=HM_REQ_SEARCH, keys=keys.ctypes.data, n=len(keys), out=out.ctypes.data)
         return Ticket(self, self._submit(r), HM_REQ_SEARCH, (keys, out), lambda: out)
 

@@ -24,8 +24,9 @@
  * hm_search_batches, hm_export, hm_search_baseline) may be issued from any
  * host threads on any streams, and their work may overlap on the device: each
  * call leases a scratch block of its own from the tree's pool, ordered on the
- * device after that block's previous use, and a block grows by a
- * stream-ordered free and allocation, never by a device-wide synchronisation.
+ * device after that block's previous use; a block that is too small is
+ * replaced by one half again as large and the old one is freed only with the
+ * tree, so no call frees device memory (which would synchronise the device).
  * Host-buffer searches of one tree take turns (they share the tree's copy
  * streams and pinned staging).  Calls that change the tree or its settings
  * (hm_upsert_batch, hm_delete_batch, hm_set_search_config, hm_autotune,
@@ -250,7 +251,10 @@ typedef struct {
   const int32_t *lens;   /* range: record counts */
   const int64_t *vals;   /* upsert: values */
   size_t n;
-  int64_t *out;          /* search: n values or -1 */
+  int64_t *out;          /* search: n values or -1.  A search's keys and out may
+                            also be page-locked host memory (cudaHostAlloc,
+                            cudaHostRegister) or device memory: those are
+                            copied by DMA with no host staging copy */
   int64_t *offsets;      /* range: n+1 offsets into out_keys/out_vals */
   int64_t *out_keys, *out_vals;
   size_t out_cap;        /* range: record capacity; HM_ECAPACITY if exceeded */
@@ -274,11 +278,12 @@ typedef struct {
   /* Where a read's time goes (searches and ranges completed since the last
    * reset, p50 and p99 of each part): queue = submitted until taken into a
    * launch (waits for slots, the memory budget and write epochs ahead of it);
-   * stage = inputs copied to pinned staging and the launch enqueued; device =
+   * stage = inputs copied to pinned staging (page-locked and device buffers
+   * skip it) and the launch enqueued; device =
    * enqueued until the launch is seen finished (copies and kernels); finish =
    * results copied to the caller's buffers.  Per write epoch, the mean wait
-   * for the launches before it to finish (drain) and the mean time to apply
-   * it. */
+   * for the kernels of the reads before it to finish (drain; their result
+   * copies may still run during the epoch) and the mean time to apply it. */
   double queue_p50_us, queue_p99_us, stage_p50_us, stage_p99_us;
   double device_p50_us, device_p99_us, finish_p50_us, finish_p99_us;
   double epoch_drain_mean_us, epoch_apply_mean_us;

@@ -3,8 +3,9 @@
 The C ABI lets read-only calls (hm_search, hm_range, hm_search_batches,
 hm_export) on one tree run concurrently on different streams, from one host
 thread or several.  Each call leases its own block of the tree's scratch pool;
-a block is ordered after its previous use, and it grows by a stream-ordered
-free and allocation, not by a device-wide synchronisation.  The bucket join's
+a block is ordered after its previous use, and a block that is too small is
+replaced by a larger one (the old one is freed with the tree), so no call
+frees device memory while others run.  The bucket join's
 boundary cache is filled once under the tree's lock, and later callers wait on
 the fill's event.
 

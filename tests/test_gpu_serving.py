@@ -3,6 +3,7 @@ continuous batching from several submitter threads, and the host-side
 failure paths (admission refusals, cancellation, timeouts, bad requests).
 No test faults or hangs the GPU: every failure is made on the host."""
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -92,6 +93,40 @@ def test_mixed_stream_results_equal_results_alone():
             check(kind, tk.wait(), e)
 
 
+def test_page_locked_buffers_mixed_with_pageable():
+    """Point requests whose keys and/or out are page-locked go by DMA, the
+    others through staging, coalesced into the same launches and around
+    upsert epochs; every answer equals the oracle's."""
+    keys, tree = make_tree(1 << 18, seed=21)
+    reqs = request_mix(keys, 200, seed=23)
+    exp, sk, sv = expected_results(keys, reqs)
+    rng = np.random.default_rng(29)
+
+    def pinned(a):
+        b = torch.empty(len(a), dtype=torch.int64, pin_memory=True).numpy()
+        b[:] = a
+        return b
+
+    kinds = []
+    with tree, Server(tree, streams=3, max_launch_queries=1 << 15) as srv:
+        tickets = []
+        for kind, data in reqs:
+            if kind == "search":
+                mode = int(rng.integers(0, 4))  # bit 0: keys pinned, bit 1: out pinned
+                kinds.append(mode)
+                q = pinned(data) if mode & 1 else data
+                out = torch.empty(len(data), dtype=torch.int64, pin_memory=True).numpy() if mode & 2 else None
+                tickets.append(srv.search(q, out=out))
+            elif kind == "range":
+                tickets.append(srv.range(*data))
+            else:
+                tickets.append(srv.upsert(*data))
+        for (kind, _), tk, e in zip(reqs, tickets, exp):
+            check(kind, tk.wait(), e)
+        assert srv.stats()["failed"] == 0
+    assert set(kinds) == {0, 1, 2, 3}
+
+
 def test_concurrent_submitters_continuous_batching():
     keys, tree = make_tree(1 << 19, seed=9)
     sk = np.sort(keys)
@@ -143,6 +178,9 @@ def test_stop_cancels_queued_and_wait_times_out():
         with pytest.raises(HarmoniaError) as e:  # still queued: a zero wait times out
             big[-1].wait(timeout_us=0)
         assert e.value.code == -7
+        t_end = time.monotonic() + 10.0  # the first request has left the queue (launched)
+        while srv.stats()["launches"] < 1 and time.monotonic() < t_end:
+            time.sleep(0.001)
         srv.stop()  # queued requests are cancelled, in-flight ones finish
         statuses = []
         for tk in big:
