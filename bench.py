@@ -234,6 +234,14 @@ def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
            "search": {"value": round(m / sec / 1e6, 3), "unit": UNIT, "ms_per_step": round(sec * 1e3, 1),
                       "sample": f"the whole {m}-query batch, median of 3"}}
     if kind == "ppi":
+        # the reference's second CPU search: 16 queries per group, AVX2 child
+        # search, each next node prefetched (search_cpu_prefetch_NTG_PPI)
+        tree.search_prefetch(q[: 1 << 20], threads)
+        sec = median_s(lambda: tree.search_prefetch(q, threads))
+        same = bool((tree.search_prefetch(q, threads) == cpu_out).all())
+        res["search_prefetch"] = {"value": round(m / sec / 1e6, 3), "unit": UNIT, "ms_per_step": round(sec * 1e3, 1),
+                                  "same_results": same,
+                                  "sample": f"the whole {m}-query batch, median of 3"}
         st, ln = dg.gen_ranges(1 << 20, 1, 256, seed=12)
         rec, _ = tree.range_timed(st, ln, threads)
         sec = median_s(lambda: tree.range_timed(st, ln, threads))
@@ -931,6 +939,13 @@ def main():
                              f"{ppi['build_s']} s excluded"}
         elif ppi:
             cpu_port["reference"] = ppi
+        if "search_prefetch" in ppi:
+            f = ppi["search_prefetch"]
+            extras["cpu_reference_prefetch"] = dict(
+                f, cores=ppi["cores"],
+                what="the reference's software-pipelined CPU search (search_cpu_prefetch_NTG_PPI, "
+                     "cpu-search-prefetch-avxNTG.cpp:480-535: 16 queries per group, AVX2 child search, "
+                     "prefetch of each next node) on the same PPI tree, OpenMP over groups")
         if "range" in ppi and "skewed_range" in extras:
             extras["skewed_range"]["range"]["cpu_reference"] = dict(ppi["range"], cores=ppi["cores"])
         if "gpu" in ppi:

@@ -229,6 +229,7 @@ def _ref_lib(path: str = REF_SO):
             getattr(lib, f).argtypes = [_P]
             getattr(lib, f).restype = _L
         lib.hmref_search.argtypes = [_P, _P, _L, _P, ctypes.c_int]
+        lib.hmref_search_prefetch.argtypes = [_P, _P, _L, _P, ctypes.c_int]
         lib.hmref_range.argtypes = [_P, _P, _P, _L, _P, _P, _P, _L]
         lib.hmref_range.restype = _L
         lib.hmref_range_between.argtypes = [_P, _P, _P, _L, _P, _P, _P, _L, ctypes.c_int]
@@ -274,6 +275,14 @@ class RefTree:
         q = np.ascontiguousarray(q, dtype=np.int64)
         out = np.empty_like(q)
         _ref_lib(self.lib_path).hmref_search(self.h, _ptr(q), len(q), _ptr(out), threads)
+        return out
+
+    def search_prefetch(self, q, threads: int = 0) -> np.ndarray:
+        """The reference's software-pipelined search (16 queries per group,
+        AVX2 child search, prefetch of each next node); fresh trees only."""
+        q = np.ascontiguousarray(q, dtype=np.int64)
+        out = np.empty_like(q)
+        _ref_lib(self.lib_path).hmref_search_prefetch(self.h, _ptr(q), len(q), _ptr(out), threads)
         return out
 
     def range(self, start, length):

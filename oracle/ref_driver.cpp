@@ -125,6 +125,51 @@ void hmref_search(void *hp, const long long *q, long n, long long *out,
   }
 }
 
+// The reference's software-pipelined CPU point search, as
+// search_cpu_prefetch_NTG_PPI runs it for 64-bit keys
+// (cpu-search-prefetch-avxNTG.cpp:480-535; that file builds only with Boost
+// and PAPI, so the loop is re-hosted here over the same tree methods): a
+// group of 16 queries descends one level at a time, four at once through
+// the tree's AVX2 child search (BPlusTree::getChildIdx_avx_4keys,
+// avx.cpp:127-190), each inner node prefetched just before the compare that
+// reads it; the last step finds the key in the big leaf's record list
+// (BLeaf_node::findKey).  OpenMP over groups; a tail of fewer than 16
+// queries takes BPlusTree::search.  Fresh trees only (no Newupdate nodes).
+void hmref_search_prefetch(void *hp, const long long *q, long n, long long *out, int threads) {
+  BPlusTree *t = static_cast<RefTree *>(hp)->ppi;
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+  constexpr int kGroup = 16;
+  const int height = t->getHeight();
+  int *prefix = t->getPrefixArray();
+  const int inner_wo_last = t->getInnerSize_wo_last_inner_node();
+  const long groups = n / kGroup;
+#pragma omp parallel for num_threads(nt) schedule(static)
+  for (long g = 0; g < groups; g++) {
+    key_t keys[kGroup];
+    int node[kGroup], rel[kGroup];
+    Inner_node *nodes[kGroup];
+    for (int i = 0; i < kGroup; i++) {
+      keys[i] = q[g * kGroup + i];
+      node[i] = 0;
+    }
+    for (int level = 1; level < height; level++) {
+      for (int b = 0; b < kGroup; b += 4) {
+        for (int j = b; j < b + 4; j++) {
+          nodes[j] = t->getInnerNodeByIdx(node[j]);
+          __builtin_prefetch(nodes[j], 0, 3);
+        }
+        t->getChildIdx_avx_4keys(&nodes[b], &keys[b], &rel[b]);
+        for (int j = b; j < b + 4; j++) node[j] = prefix[node[j]] + rel[j];
+      }
+    }
+    for (int i = 0; i < kGroup; i++) {
+      BLeaf_node *leaf = t->getBLeafNodeByIdx(t->getInnerNodeIdx(nodes[i]) - inner_wo_last);
+      out[g * kGroup + i] = leaf->findKey(rel[i], keys[i]);
+    }
+  }
+  for (long i = groups * kGroup; i < n; i++) out[i] = t->search(q[i]);
+}
+
 // Timing form of the range scan, as the reference's CPU range experiment
 // runs it (OpenMP over blocks of SWP_P2 = 1000 queries, cpu-range.cpp:80-88):
 // every query walks its records into a per-thread buffer (the reference

@@ -147,6 +147,19 @@ def test_port_matches_reference_directly(n, fanout, leaf_cap):
     assert all((x == y).all() for x, y in zip(a, b))
 
 
+@pytest.mark.skipif(not po.ref_available(), reason="reference library not built in this checkout")
+@pytest.mark.parametrize("n", [5, 100, 5000, 1 << 16])
+def test_reference_prefetch_search_equals_its_plain_search(n):
+    """The reference's software-pipelined CPU search (timed as a second CPU
+    figure) answers as its plain search does, including a ragged tail."""
+    keys = dg.gen_keys(n, seed=300 + n)
+    ref = po.RefTree(keys, dg.values_for(keys))
+    q = dg.gen_point_queries(keys, 20003, 0.5, seed=n)
+    q[:3] = [keys.min(), keys.max(), -7]
+    assert (ref.search_prefetch(q) == ref.search(q)).all()
+    assert (ref.search_prefetch(q, threads=3) == ref.search(q)).all()
+
+
 def test_port_matches_c1_range_between_digests(c1):
     """Inclusive ranges (BPlusTree::range_search) before and after the first
     C1 upsert epoch, on two layouts of the restatement."""
