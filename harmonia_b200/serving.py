@@ -65,6 +65,10 @@ def _bind():
     return L
 
 
+def _is_cuda_tensor(a) -> bool:
+    return getattr(a, "is_cuda", False) is True and hasattr(a, "data_ptr")
+
+
 class Ticket:
     def __init__(self, server: "Server", ticket: int, kind: int, keep: tuple, result):
         self.server = server
@@ -114,13 +118,39 @@ class Server:
     def search(self, keys, out=None) -> Ticket:
         """Point search; out (optional) receives the values.  keys and out in
         page-locked memory (e.g. numpy views of torch tensors made with
-        pin_memory=True) are copied by DMA without a staging copy."""
+        pin_memory=True) are copied by DMA without a staging copy; so are
+        contiguous int64 torch CUDA tensors (device memory), which may be
+        passed for either."""
+        if _is_cuda_tensor(keys) or _is_cuda_tensor(out):
+            return self._search_tensors(keys, out)
         keys = np.ascontiguousarray(keys, dtype=np.int64)
         if out is None:
             out = np.empty(len(keys), np.int64)
         elif out.dtype != np.int64 or not out.flags.c_contiguous or len(out) != len(keys):
             raise ValueError("out must be a contiguous int64 array as long as keys")
         r = Request(kind=HM_REQ_SEARCH, keys=keys.ctypes.data, n=len(keys), out=out.ctypes.data)
+        return Ticket(self, self._submit(r), HM_REQ_SEARCH, (keys, out), lambda: out)
+
+    def _search_tensors(self, keys, out):
+        import torch
+        if not _is_cuda_tensor(keys):
+            keys = np.ascontiguousarray(keys, dtype=np.int64)
+        n = len(keys)
+        if out is None:
+            out = np.empty(n, np.int64)
+        for a in (keys, out):
+            if _is_cuda_tensor(a):
+                if a.dtype != torch.int64 or not a.is_contiguous():
+                    raise ValueError("CUDA tensors must be contiguous int64")
+            elif a.dtype != np.int64 or not a.flags.c_contiguous:
+                raise ValueError("host buffers must be contiguous int64 arrays")
+        if len(out) != n:
+            raise ValueError("out must be as long as keys")
+
+        def ptr(a):
+            return a.data_ptr() if _is_cuda_tensor(a) else a.ctypes.data
+
+        r = Request(kind=HM_REQ_SEARCH, keys=ptr(keys), n=n, out=ptr(out))
         return Ticket(self, self._submit(r), HM_REQ_SEARCH, (keys, out), lambda: out)
 
     def range(self, start, length, cap=None) -> Ticket:

@@ -203,6 +203,34 @@ def test_search_batches_large_presorted_union(c1):
     t.set_search_config(sort_bits=-1)
 
 
+def test_search_batches_bucket_join_placed(c1):
+    """A batch set through the bucket join with results placed in first-pass
+    order (total under 2^25 queries): the first pass reads every batch in
+    place, the join writes first-pass positions, the one inverse pass writes
+    each batch's output; the same through a captured plan."""
+    keys, sk, t = c1
+    oracle = po.PortTree(sk, dg.values_for(sk))
+    sizes = [1 << 20, 1000, 1 << 19, 5, 777777, 8192, 8193]
+    qs = [cuda(dg.gen_point_queries(keys, m, 0.6, seed=500 + i)) for i, m in enumerate(sizes)]
+    outs = [torch.full((len(q),), -77, dtype=torch.int64, device="cuda") for q in qs]
+    t.set_search_config(join=1)
+    try:
+        t.search_batches(list(zip(qs, outs)))
+        for q, o in zip(qs, outs):
+            assert (o.cpu().numpy() == oracle.search(q.cpu().numpy())).all()
+        plan = t.plan(list(zip(qs, outs)))
+        for rep in range(2):
+            for o in outs:
+                o.fill_(-77)
+            plan.launch()
+            torch.cuda.synchronize()
+            for q, o in zip(qs, outs):
+                assert (o.cpu().numpy() == oracle.search(q.cpu().numpy())).all(), rep
+        plan.close()
+    finally:
+        t.set_search_config(join=-1)
+
+
 def test_plan_replay_matches_and_follows_rebuild():
     keys = dg.gen_keys(1 << 18, seed=61)
     vals = dg.values_for(keys)

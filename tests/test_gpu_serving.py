@@ -127,6 +127,26 @@ def test_page_locked_buffers_mixed_with_pageable():
     assert set(kinds) == {0, 1, 2, 3}
 
 
+def test_device_buffers():
+    """Point requests whose keys and/or out are CUDA tensors (device memory)
+    are copied by DMA (device to device), mixed with host requests."""
+    keys, tree = make_tree(1 << 18, seed=31)
+    sk = np.sort(keys)
+    oracle = po.PortTree(sk, dg.values_for(sk))
+    with tree, Server(tree, streams=2, max_launch_queries=1 << 15) as srv:
+        qs = [dg.gen_point_queries(keys, 1000 + 111 * i, 0.7, seed=40 + i) for i in range(12)]
+        tks, outs = [], []
+        for i, q in enumerate(qs):
+            mode = i % 4  # bit 0: keys on the device, bit 1: out on the device
+            kq = torch.from_numpy(q).cuda() if mode & 1 else q
+            out = torch.empty(len(q), dtype=torch.int64, device="cuda") if mode & 2 else None
+            tks.append(srv.search(kq, out=out))
+        for q, tk in zip(qs, tks):
+            got = tk.wait()
+            got = got.cpu().numpy() if hasattr(got, "cpu") else got
+            assert (got == oracle.search(q)).all()
+
+
 def test_concurrent_submitters_continuous_batching():
     keys, tree = make_tree(1 << 19, seed=9)
     sk = np.sort(keys)
