@@ -927,23 +927,20 @@ int hm_delete_batch(hm_tree *t, const int64_t *keys, size_t n_, size_t *removed,
   if (n == 0) return HM_OK;
   cudaStream_t s = as_stream(hs);
   const int64_t *dk = keys;
-  int64_t *tmp = nullptr;
+  ScratchLease staging(t, s);  // host batches are copied into a leased block (no cudaFree)
   if (!is_device_ptr(keys)) {
-    cudaError_t e = cudaMalloc(&tmp, (size_t)align_up(n * 8, 256));
+    int rc = staging.acquire((size_t)align_up(n * 8, 256));
+    if (rc) return rc;
+    int64_t *tk = static_cast<int64_t *>(staging.ptr());
+    cudaError_t e = cudaMemcpyAsync(tk, keys, n * 8, cudaMemcpyDefault, s);
     if (e != cudaSuccess) return cuda_err(e);
-    e = cudaMemcpyAsync(tmp, keys, n * 8, cudaMemcpyDefault, s);
-    if (e != cudaSuccess) {
-      cudaFree(tmp);
-      return cuda_err(e);
-    }
-    dk = tmp;
+    dk = tk;
   }
   int64_t gone = 0;
   int tok = prof_begin(t, s);
   int rc = delete_epoch(t, dk, n, &gone, s);
   prof_end(t, kStageDelete, tok, s);
   cudaError_t e = cudaStreamSynchronize(s);
-  if (tmp) cudaFree(tmp);
   if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
   if (removed) *removed = (size_t)gone;
   choose_smem_levels(t);
@@ -958,25 +955,22 @@ int hm_upsert_batch(hm_tree *t, const int64_t *keys, const int64_t *vals, size_t
   if (n == 0) return HM_OK;
   cudaStream_t s = as_stream(hs);
   const int64_t *dk = keys, *dv = vals;
-  int64_t *tmp = nullptr;
+  ScratchLease staging(t, s);  // host batches are copied into a leased block (no cudaFree)
   if (!(is_device_ptr(keys) && is_device_ptr(vals))) {
-    cudaError_t e = cudaMalloc(&tmp, 2 * (size_t)align_up(n * 8, 256));
-    if (e != cudaSuccess) return cuda_err(e);
-    int64_t *tv = reinterpret_cast<int64_t *>(reinterpret_cast<char *>(tmp) + align_up(n * 8, 256));
-    e = cudaMemcpyAsync(tmp, keys, n * 8, cudaMemcpyDefault, s);
+    int rc = staging.acquire(2 * (size_t)align_up(n * 8, 256));
+    if (rc) return rc;
+    int64_t *tk = static_cast<int64_t *>(staging.ptr());
+    int64_t *tv = reinterpret_cast<int64_t *>(static_cast<char *>(staging.ptr()) + align_up(n * 8, 256));
+    cudaError_t e = cudaMemcpyAsync(tk, keys, n * 8, cudaMemcpyDefault, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(tv, vals, n * 8, cudaMemcpyDefault, s);
-    if (e != cudaSuccess) {
-      cudaFree(tmp);
-      return cuda_err(e);
-    }
-    dk = tmp;
+    if (e != cudaSuccess) return cuda_err(e);
+    dk = tk;
     dv = tv;
   }
   int tok = prof_begin(t, s);
   int rc = upsert_epoch(t, dk, dv, n, flags, s);
   prof_end(t, kStageUpsert, tok, s);
   cudaError_t e = cudaStreamSynchronize(s);
-  if (tmp) cudaFree(tmp);
   if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
   choose_smem_levels(t);
   return rc ? rc : hm_sync(t, hs);

@@ -150,6 +150,192 @@ __global__ void __launch_bounds__(1024) small_sort_unique_kernel(const int64_t *
   if (tid == blockDim.x - 1) *count = before;
 }
 
+// ---- small epochs in one kernel ----
+//
+// An epoch of at most kSmallEpoch keys (the serving loop's write requests)
+// whose new keys all fit their leaves is applied by one CTA: bitonic sort of
+// (key, input index) in shared memory, last occurrence kept, a descent per
+// key, hits written in place, each leaf's new keys merged into its sorted row
+// from the back; a second kernel adds the new keys to leaf_base.  The CTA
+// checks everything (Max_Key, room in every touched leaf) before it writes
+// anything, so an epoch it cannot apply leaves the tree untouched for the
+// general path.  Same results as the general path, one host synchronisation
+// instead of four.
+constexpr int kSmallEpoch = 1024;
+
+struct SmallEpochResult {
+  int32_t applied;   // 1: applied in place; 0: nothing changed
+  int32_t maxkey;    // a key equals Max_Key (nothing changed)
+  int32_t inserted;  // new keys
+  int32_t runs;      // leaves that received new keys
+  int64_t new_min, new_max;  // smallest and largest new key
+};
+
+__global__ void __launch_bounds__(kSmallEpoch) small_epoch_kernel(
+    DevTree t, int f, int lc, int li, int flags, const int64_t *__restrict__ keys, const int64_t *__restrict__ vals,
+    int n, int64_t *leaf_rows, int32_t *leaf_cnt, int32_t *__restrict__ run_leaf, int32_t *__restrict__ run_pre,
+    SmallEpochResult *__restrict__ res) {
+  __shared__ uint64_t sk[kSmallEpoch];
+  __shared__ int32_t si[kSmallEpoch];
+  __shared__ int64_t kk[kSmallEpoch], kv[kSmallEpoch];  // kept keys and values, key order
+  __shared__ int32_t lf[kSmallEpoch];                     // their leaves; then the misses' leaves
+  __shared__ int32_t wsum[32];
+  __shared__ int32_t total;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // exclusive block scan of one int per thread; total of all in `total`
+  auto scan = [&](int v) {
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    __syncthreads();
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int before = incl - v;
+    for (int w = 0; w < warp; w++) before += wsum[w];
+    if (tid == blockDim.x - 1) total = before + v;
+    __syncthreads();
+    return before;
+  };
+  int P = 1;
+  while (P < n) P <<= 1;
+  bool mx = false;
+  for (int i = tid; i < P; i += blockDim.x) {
+    const bool real = i < n;
+    const int64_t k = real ? keys[i] : 0;
+    mx |= real && k == kMaxKey;
+    sk[i] = real ? (uint64_t)k ^ kSign : ~0ull;  // padding sorts after every real key
+    si[i] = real ? i : INT32_MAX;
+  }
+  if (__syncthreads_or(mx)) {
+    if (tid == 0) res->maxkey = 1;
+    return;
+  }
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < P; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const bool asc = (i & k) == 0;
+          const bool gt = sk[i] > sk[ixj] || (sk[i] == sk[ixj] && si[i] > si[ixj]);
+          if (gt == asc) {
+            const uint64_t tk = sk[i];
+            sk[i] = sk[ixj];
+            sk[ixj] = tk;
+            const int32_t ti = si[i];
+            si[i] = si[ixj];
+            si[ixj] = ti;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // keep each key's last occurrence (thread i owns sorted element i)
+  const bool keep = tid < n && (tid == n - 1 || sk[tid] != sk[tid + 1]);
+  const int at = scan(keep);
+  const int m = total;
+  if (keep) {
+    kk[at] = (int64_t)(sk[tid] ^ kSign);
+    kv[at] = vals[si[tid]];
+  }
+  __syncthreads();
+  // descend: hit slot or miss, per kept key (thread i owns kept key i)
+  int64_t key = 0, val = 0;
+  int32_t leaf = -1, slot = -1;
+  const int stride = li + 2 * lc;
+  if (tid < m) {
+    key = kk[tid];
+    val = kv[tid];
+    leaf = descend_leaf(t, f, key);
+    const int64_t *kr = t.leaf_rows + (int64_t)leaf * stride + li;
+    const int cnt = t.leaf_cnt[leaf];
+    for (int x = 0; x < cnt; x++)
+      if (kr[x] == key) slot = x;
+  }
+  const bool miss = tid < m && slot < 0;
+  const int mi = scan(miss);
+  const int nm = total;
+  if (miss) {  // the misses, still in key order, compacted
+    kk[mi] = key;
+    kv[mi] = val;
+    lf[mi] = leaf;
+  }
+  __syncthreads();
+  // runs of misses per leaf, and room for each run
+  bool start = false, fits = true;
+  int rl = 0;
+  if (tid < nm) {
+    start = tid == 0 || lf[tid] != lf[tid - 1];
+    if (start) {
+      int e = tid + 1;
+      while (e < nm && lf[e] == lf[tid]) e++;
+      rl = e - tid;
+      fits = t.leaf_cnt[lf[tid]] + rl <= lc;
+    }
+  }
+  if (!__syncthreads_and(fits)) return;  // res->applied stays 0: nothing changed
+  // hits in place (before the merges, which move the rows' values)
+  if (tid < m && slot >= 0)
+    leaf_rows[(int64_t)leaf * stride + li + lc + slot] = (flags & HM_UPSERT_REF_KEY_MINUS_1) ? key - 1 : val;
+  __syncthreads();
+  const int r = scan(start);
+  const int runs = total;
+  if (start) {
+    // merge the run [tid, tid + rl) into the leaf's sorted row from the back
+    const int32_t L = lf[tid];
+    int64_t *kr = leaf_rows + (int64_t)L * stride + li;
+    int64_t *vr = kr + lc;
+    int a = leaf_cnt[L], b = rl;
+    for (int o = a + b - 1; o >= 0 && b > 0; o--) {
+      if (a > 0 && kr[a - 1] > kk[tid + b - 1]) {
+        kr[o] = kr[a - 1];
+        vr[o] = vr[a - 1];
+        a--;
+      } else {
+        kr[o] = kk[tid + b - 1];
+        vr[o] = kv[tid + b - 1];
+        b--;
+      }
+    }
+    const int nc = leaf_cnt[L] + rl;
+    if (li > 0) {
+      int64_t *ir = leaf_rows + (int64_t)L * stride;
+      for (int x = 0; x < li; x++) ir[x] = (8 * (x + 1) < nc) ? kr[8 * (x + 1)] : kMaxKey;
+    }
+    leaf_cnt[L] = nc;
+    run_leaf[r] = L;
+    run_pre[r] = tid;  // new keys in earlier runs (the misses before this run)
+  }
+  if (tid == 0) {
+    res->applied = 1;
+    res->inserted = nm;
+    res->runs = runs;
+    if (nm > 0) {
+      res->new_min = kk[0];
+      res->new_max = kk[nm - 1];
+    }
+  }
+}
+
+// leaf_base[l] += new keys in leaves before l, after an applied small epoch.
+__global__ void small_epoch_base_kernel(int64_t *leaf_base, int64_t n_leaf, const int32_t *__restrict__ run_leaf,
+                                        const int32_t *__restrict__ run_pre, const SmallEpochResult *__restrict__ res) {
+  if (!res->applied || res->inserted == 0) return;
+  const int runs = res->runs, inserted = res->inserted;
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < n_leaf; l += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = runs;  // first run whose leaf >= l
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (run_leaf[mid] < l) lo = mid + 1; else hi = mid;
+    }
+    const int add = lo < runs ? run_pre[lo] : inserted;
+    if (add) leaf_base[l] += add;
+  }
+}
+
 // Hits are updated in place; misses get miss[i] = 1 and their leaf.
 __global__ void apply_kernel(DevTree t, int f, int lc, int li, int flags,
                              const int64_t *__restrict__ bk, const int64_t *__restrict__ bv, int64_t m,
@@ -546,6 +732,37 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
                  cudaStream_t s) {
   if (n <= 0) return HM_OK;
   const int lc = t->cfg.leaf_cap, li = t->leaf_index, f = t->cfg.fanout;
+  if (n <= kSmallEpoch && t->n_keys > 0) {  // one kernel, one synchronisation, if every new key fits
+    ScratchLease lease(t, s);
+    const size_t rb = al(4 * n);
+    int rc = lease.acquire(2 * rb + al(sizeof(SmallEpochResult)) + 256);
+    if (rc) return rc;
+    char *p = static_cast<char *>(lease.ptr());
+    int32_t *run_leaf = reinterpret_cast<int32_t *>(p);
+    int32_t *run_pre = reinterpret_cast<int32_t *>(p + rb);
+    SmallEpochResult *dres = reinterpret_cast<SmallEpochResult *>(p + 2 * rb);
+    SmallEpochResult hres{};
+    cudaError_t e = cudaMemsetAsync(dres, 0, sizeof(SmallEpochResult), s);
+    if (e != cudaSuccess) return cuda_err(e);
+    small_epoch_kernel<<<1, kSmallEpoch, 0, s>>>(t->view(), f, lc, li, flags, d_keys, d_vals, (int)n, t->leaf_rows,
+                                                 t->leaf_cnt, run_leaf, run_pre, dres);
+    small_epoch_base_kernel<<<grid_for(t->n_leaf), kThreads, 0, s>>>(t->leaf_base, t->n_leaf, run_leaf, run_pre,
+                                                                     dres);
+    note_launch(2);
+    e = cudaMemcpyAsync(&hres, dres, sizeof(hres), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_err(e);
+    if (hres.maxkey) return HM_EMAXKEY;
+    if (hres.applied) {
+      t->n_keys += hres.inserted;
+      if (hres.inserted > 0) {
+        if (hres.new_min < t->key_min) t->key_min = hres.new_min;
+        if (hres.new_max > t->key_max) t->key_max = hres.new_max;
+      }
+      return HM_OK;
+    }
+    // some leaf has no room: nothing was changed; the general path below
+  }
   // scratch: uk, uk_alt, idx, idx_alt (n each, 8 B), keep/miss/leaf_of/is_start (4 B),
   // at (8 B, n+1), bk, bv, mk, mv, run_start (8 B), run_len/run_leaf/ml (4 B), sort scratch, flags
   const size_t s8 = al(8 * (n + 1)), s4 = al(4 * (n + 1));

@@ -118,6 +118,58 @@ def test_tiny_batches_on_a_large_tree():
         assert all((a == b).all() for a, b in zip(got, exp))
 
 
+@pytest.mark.parametrize("fanout,leaf_cap,fill", [(64, 16, 12), (128, 64, 48)])
+def test_small_epochs_one_kernel_path(fanout, leaf_cap, fill):
+    """Epochs of at most 1024 keys go through the one-kernel path when every
+    new key fits its leaf, and fall back to the general path (untouched tree
+    first) when one does not: duplicates, both value rules, new smallest and
+    largest keys (the join's bucket range moves), a full leaf, ranges and
+    searches through the descent and the bucket join after every epoch."""
+    keys = dg.gen_keys(1 << 18, seed=91)
+    sk, sv = np.sort(keys), dg.values_for(np.sort(keys))
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), fanout=fanout, leaf_cap=leaf_cap,
+                             leaf_fill=fill) as t:
+        lo, hi = int(sk[0]), int(sk[-1])
+        crowd = np.arange(int(sk[100]) + 1, int(sk[100]) + 1 + 3 * leaf_cap, dtype=np.int64)  # overflows one leaf
+        crowd = crowd[~np.isin(crowd, sk)][:leaf_cap]
+        epochs = [
+            (dg.gen_upserts(sk, 1000, 0.5, seed=92), 0),
+            ((np.array([lo - 5, hi + 5, lo - 5, int(sk[7])], np.int64), np.array([1, 2, 3, 4], np.int64)), 0),
+            (dg.gen_upserts(sk, 64, 0.3, seed=93), 1),
+            ((crowd, crowd + 7), 0),
+            (dg.gen_upserts(sk, 1024, 0.6, seed=94), 1),
+        ]
+        for (bk, bv), ref in epochs:
+            if ref:
+                t.insert_parallel_Newupdate_batch(bk, bv)
+                bv = np.where(np.isin(bk, sk), bk - 1, bv)
+                # the reference rule: an existing key's value becomes key - 1
+                last = {}
+                for k, v in zip(bk.tolist(), bv.tolist()):
+                    last[k] = v
+                bk = np.array(list(last.keys()), np.int64)
+                bv = np.array(list(last.values()), np.int64)
+            else:
+                t.upsert(cuda(bk), cuda(bv))
+            sk, sv = po.upsert_set(sk, sv, bk, bv)
+            xk, xv = t.export()
+            assert (xk == sk).all() and (xv == sv).all()
+            oracle = po.PortTree(sk, sv)
+            q = np.concatenate([bk, dg.gen_point_queries(sk, 1 << 18, 0.7, seed=95), [sk[0] - 1, sk[-1] + 1]])
+            for join in (2, 1):
+                t.set_search_config(join=join)
+                assert (t.search(cuda(q)).cpu().numpy() == oracle.search(q)).all(), join
+            t.set_search_config(join=-1)
+            st, ln = dg.gen_ranges(500, 1, 100, seed=96)
+            st[:3] = [sk[0], sk[-1], bk[0]]
+            got = t.range_search(st, ln)
+            assert all((a == b).all() for a, b in zip(got, oracle.range(st, ln)))
+            room = np.int64(2**63 - 2) - st  # inclusive ranges rank their ends through leaf_base
+            en = st + np.minimum(room, np.int64(1) << 44)
+            got = t.range_between(st, en)
+            assert all((a == b).all() for a, b in zip(got, oracle.range_between(st, en)))
+
+
 @pytest.mark.parametrize("fanout,leaf_cap,fill", [(64, 16, 12), (128, 64, 48), (64, 64, 40)])
 def test_overflowing_leaf_rebalances_its_subtree(fanout, leaf_cap, fill):
     # new keys packed into one leaf's key range overflow it while its subtree
