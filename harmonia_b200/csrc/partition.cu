@@ -233,14 +233,9 @@ __global__ void __launch_bounds__(kThreads) psa_hist_kernel(const int64_t *__res
 constexpr int kSc = HM_PSA_SCATTER_THREADS;
 constexpr int kPer = kTile / kSc;
 static_assert(kSc >= 256 && kTile % kSc == 0 && kChunk % kTile == 0, "a thread per digit; positions in 16 bits");
-// Ranking inside a tile: 0 = a shared-memory atomic per key on the tile's
-// 256 digit counters; 1 = per warp, __match_any_sync finds the lanes with the
-// same digit, the lowest of them adds their count to the warp's own counter
-// (no atomics), and a scan over the warps turns the warp counters into offsets.
-#ifndef HM_PSA_RANK_MATCH
-#define HM_PSA_RANK_MATCH 0
-#endif
-constexpr int kScWarps = kSc / 32;
+// Ranking inside a tile: a shared-memory atomic per key on the tile's 256
+// digit counters (measured faster than warp-level __match_any_sync ranking
+// into per-warp counters).
 constexpr int stage_bytes() { return kTile * 12; }
 
 template <typename T, bool LOAD, bool BATCHED>
@@ -254,9 +249,6 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(
   uint32_t *saux = reinterpret_cast<uint32_t *>(dyn + 8 * kTile);  // digit << 16 | tile position
   __shared__ unsigned cnt[256];
   __shared__ unsigned tstart[256];
-#if HM_PSA_RANK_MATCH
-  __shared__ uint16_t wcnt[kScWarps][256];  // per warp and digit: count, then offset among the warps
-#endif
   __shared__ int64_t gcur[256];
   __shared__ int64_t adj[256];
   __shared__ unsigned wsum[8];
@@ -281,44 +273,11 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(
   int64_t t0 = c.begin;
   for (;;) {
     const bool last_tile = t0 + kTile >= c.end;
-#if HM_PSA_RANK_MATCH
-    for (int x = tid; x < kScWarps * 256; x += kSc) (&wcnt[0][0])[x] = 0;
-#else
     if (digit_thread) cnt[tid] = 0;
-#endif
     if (tid == 0 && last_tile) next_chunk = (int)gridDim.x + atomicAdd(&nchunks_total[1], 1);
     __syncthreads();
     const int n = (int)min((int64_t)kTile, c.end - t0);
     unsigned dr[kPer];  // digit << 16 | rank inside the tile's digit run; ~0u past the end
-#if HM_PSA_RANK_MATCH
-    const unsigned below_mask = (1u << lane) - 1u;
-#pragma unroll
-    for (int j = 0; j < kPer; j++) {
-      const bool valid = j * kSc + tid < n;
-      const unsigned d = valid ? (unsigned)((bk(k[j]) >> shift2) & mask2) : 256u;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
-      const int leader = __ffs(peers) - 1;
-      unsigned base = 0;
-      if (valid && lane == leader) {
-        base = wcnt[w][d];
-        wcnt[w][d] = (uint16_t)(base + __popc(peers));
-      }
-      base = __shfl_sync(0xffffffffu, base, leader);
-      __syncwarp();
-      dr[j] = valid ? (d << 16 | (base + __popc(peers & below_mask))) : ~0u;  // rank among the warp's keys of d
-    }
-    __syncthreads();
-    if (digit_thread) {  // per digit: offsets of the warps' runs, and the tile's count
-      unsigned run = 0;
-#pragma unroll
-      for (int x = 0; x < kScWarps; x++) {
-        const unsigned c = wcnt[x][tid];
-        wcnt[x][tid] = (uint16_t)run;
-        run += c;
-      }
-      cnt[tid] = run;
-    }
-#else
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
       if (j * kSc + tid < n) {
@@ -328,7 +287,6 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(
         dr[j] = ~0u;
       }
     }
-#endif
     __syncthreads();
     // exclusive scan of the 256 tile counts (one per digit thread)
     unsigned mine = 0, incl = 0;
@@ -354,11 +312,7 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(
     for (int j = 0; j < kPer; j++) {
       if (dr[j] != ~0u) {
         const unsigned d = dr[j] >> 16;
-#if HM_PSA_RANK_MATCH
-        const unsigned sl = tstart[d] + wcnt[w][d] + (dr[j] & 0xffffu);
-#else
         const unsigned sl = tstart[d] + (dr[j] & 0xffffu);
-#endif
         skey[sl] = k[j];
         saux[sl] = d << 16 | (unsigned)(j * kSc + tid);
       }
@@ -404,7 +358,7 @@ __global__ void __launch_bounds__(kSc, HM_PSA_SCATTER_MINB) psa_scatter_kernel(
   }
 }
 
-// Inverse of one pass for 64-bit results: CTA per input chunk.  The chunk's
+// Inverse of one pass for 64-bit results, per input chunk.  The chunk's
 // elements sit in one contiguous run per digit (offs gives the run starts, in
 // [bucket][digit][chunk] order, so the next entry ends the run); each carries
 // its offset inside the chunk.  The results are placed by offset in shared
@@ -422,104 +376,12 @@ constexpr int kRevBatch = HM_PSA_REV_BATCH;
 constexpr int kUnit = HM_PSA_REV_UNIT;
 constexpr int kUnitPer = kUnit / 32;
 
-template <bool BATCHED>
-__global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_kernel(
-    const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total, const int64_t *__restrict__ offs,
-    int nd, const int64_t *__restrict__ res_in, const uint16_t *__restrict__ loc, int64_t *__restrict__ res_out,
-    BatchView bv, const ChunkIO *__restrict__ cio) {
-  pdl_enter();
-  extern __shared__ __align__(16) int64_t staged[];  // kChunk results
-  __shared__ int64_t rs[256];
-  __shared__ int32_t rl[256];
-  __shared__ int32_t up[257];  // first unit of each run
-  __shared__ uint8_t unit_run[kChunk / kUnit + 256];
-  __shared__ int32_t wsum[8];
-  if ((int)blockIdx.x >= *nchunks_total) return;
-  const Chunk c = chunks[blockIdx.x];
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const int len = (int)(c.end - c.begin);
-  int64_t *dst = BATCHED ? cio[blockIdx.x].obase : res_out;  // a chunk lies inside one batch
-  if (tid < 256) {  // run of digit tid: start, length, units; exclusive scan of the units
-    int32_t u = 0;
-    if (tid < nd) {
-      const int64_t k = count_index(c, tid);
-      const int64_t a = offs[k];
-      const int32_t n = (int32_t)(offs[k + 1] - a);
-      rs[tid] = a;
-      rl[tid] = n;
-      u = (n + kUnit - 1) / kUnit;
-    }
-    int32_t incl = u;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    if (lane == 31) wsum[wid] = incl;
-    up[tid] = incl - u;  // within the warp, completed below
-  }
-  __syncthreads();
-  if (tid < 256) {
-    int32_t add = 0;
-    for (int x = 0; x < wid; x++) add += wsum[x];
-    up[tid] += add;
-    if (tid == 255) up[256] = up[255] + (255 < nd ? (rl[255] + kUnit - 1) / kUnit : 0);
-  }
-  __syncthreads();
-  const int units = up[nd];
-  for (int d = tid; d < nd; d += kRevThreads)  // the run of every unit
-    for (int u = up[d]; u < up[d + 1]; u++) unit_run[u] = (uint8_t)d;
-  __syncthreads();
-  // Each result goes straight from global memory to its slot in shared memory
-  // (cp.async, 8 B) once its offset is known: only the offsets pass through
-  // registers, so a warp keeps the copies of many units in flight.
-  for (int u0 = wid; u0 < units; u0 += kRevWarps * kRevBatch) {
-    uint16_t l[kRevBatch][kUnitPer];
-    int64_t a[kRevBatch];
-    int cnt[kRevBatch];
-#pragma unroll
-    for (int x = 0; x < kRevBatch; x++) {
-      const int u = u0 + x * kRevWarps;
-      cnt[x] = 0;
-      a[x] = 0;
-      if (u < units) {
-        const int d = unit_run[u];
-        const int e0 = (u - up[d]) * kUnit;
-        a[x] = rs[d] + e0;
-        cnt[x] = min(kUnit, rl[d] - e0);
-#pragma unroll
-        for (int h = 0; h < kUnitPer; h++)
-          if (lane + 32 * h < cnt[x]) l[x][h] = __ldg(loc + a[x] + lane + 32 * h);
-      }
-    }
-#pragma unroll
-    for (int x = 0; x < kRevBatch; x++)
-#pragma unroll
-      for (int h = 0; h < kUnitPer; h++)
-        if (lane + 32 * h < cnt[x]) cp_async8(staged + l[x][h], res_in + a[x] + lane + 32 * h);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  int64_t *o = dst + c.begin;
-  if ((reinterpret_cast<uintptr_t>(o) & 15) == 0) {  // 16-B stores, the odd tail element alone
-    const int pairs = len >> 1;
-    const longlong2 *sv = reinterpret_cast<const longlong2 *>(staged);
-    longlong2 *ov = reinterpret_cast<longlong2 *>(o);
-    for (int x = tid; x < pairs; x += kRevThreads) ov[x] = sv[x];
-    if ((len & 1) && tid == 0) o[len - 1] = staged[len - 1];
-  } else {
-    for (int x = tid; x < len; x += kRevThreads) o[x] = staged[x];
-  }
-}
-
-// Persistent form of the inverse (HM_PSA_REV_PERSIST): CTAs take chunks
-// blockIdx.x, blockIdx.x + gridDim.x, ...; the next chunk's descriptor, run
-// table and output pointer are loaded into registers while the current
-// chunk's result copies are in flight, which takes two dependent round trips
-// off every chunk but the first.  The per-chunk work is the same as above.
-#ifndef HM_PSA_REV_PERSIST
-#define HM_PSA_REV_PERSIST 1  // measured: both inverse passes 0.178 -> 0.169 ms at 2^24 queries
-#endif
+// Persistent CTAs take chunks blockIdx.x, blockIdx.x + gridDim.x, ...; the
+// next chunk's descriptor, run table and output pointer are loaded into
+// registers while the current chunk's result copies are in flight, which
+// takes two dependent round trips off every chunk but the first (measured:
+// both inverse passes 0.178 -> 0.169 ms at 2^24 queries against one CTA per
+// chunk).
 template <bool BATCHED>
 __global__ void __launch_bounds__(kRevThreads, HM_PSA_REV_MINB) psa_unpermute_persist_kernel(
     const Chunk *__restrict__ chunks, const int32_t *__restrict__ nchunks_total, const int64_t *__restrict__ offs,
@@ -832,16 +694,10 @@ int device_sms() {
 template <bool BATCHED = false>
 void unpermute_pass(const Pass &ps, int nd, const int64_t *res_in, const uint16_t *loc, int64_t *res_out,
                     cudaStream_t s, const BatchView &bv = BatchView(), const ChunkIO *cio = nullptr) {
-#if HM_PSA_REV_PERSIST
   opt_in_smem((const void *)psa_unpermute_persist_kernel<BATCHED>, (int)(8 * kChunk));
   const unsigned grid = (unsigned)std::min<int64_t>(ps.mc, (int64_t)device_sms() * HM_PSA_REV_MINB);
   launch_pdl(psa_unpermute_persist_kernel<BATCHED>, grid, kRevThreads, 8 * kChunk, s, ps.chunks, ps.nchunks, ps.offs,
              nd, res_in, loc, res_out, bv, cio);
-#else
-  opt_in_smem((const void *)psa_unpermute_kernel<BATCHED>, (int)(8 * kChunk));
-  launch_pdl(psa_unpermute_kernel<BATCHED>, (unsigned)ps.mc, kRevThreads, 8 * kChunk, s, ps.chunks, ps.nchunks, ps.offs, nd,
-                                                                                 res_in, loc, res_out, bv, cio);
-#endif
   note_launch();
 }
 
