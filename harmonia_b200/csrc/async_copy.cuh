@@ -1,4 +1,4 @@
-// mbarrier and 1-D bulk-copy (TMA) helpers in inline PTX, shared by the
+// mbarrier, 1-D bulk-copy and 2-D tiled (TMA) helpers in inline PTX, shared by the
 // kernels that stage global memory in shared memory.  Every wait is bounded.
 #pragma once
 
@@ -56,6 +56,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// 2-D tiled TMA load of one box of the tensor map at tmap (the address of a
+// __grid_constant__ kernel parameter) at element coordinates (x, y) into
+// shared memory; completion is counted on bar.  No multicast.  x times the
+// element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d(void *dst, const void *tmap, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Orders this thread's earlier generic-proxy accesses to shared memory
+// before later async-proxy (TMA) writes to it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 }  // namespace hm

@@ -215,11 +215,12 @@ int hm_get_config(const hm_tree *t, hm_config *cfg);
 int hm_autotune(hm_tree *t, const int64_t *sample_q, size_t n, hm_config *best);
 
 /* Polls a search kernel makes while it waits for the top levels it stages in
- * shared memory, before it gives up, records HM_ETIMEOUT (reported by
- * hm_sync) and returns without results (default 2^24, far above the
- * microseconds a copy takes).  A CTA that gave up still waits, with the
- * default bound, for its copy to land before it exits.  For tests of the
- * timeout path: 0 makes every staged wait give up at once.  Not thread-safe
+ * shared memory (and the bucket join for the leaf records its TMA loads
+ * stage), before it gives up, records HM_ETIMEOUT (reported by hm_sync) and
+ * returns without results (default 2^24, far above the microseconds a copy
+ * takes).  A CTA that gave up still waits, with the default bound, for its
+ * copies to land before it exits.  For tests of the timeout path: 0 makes
+ * every staged wait give up at once.  Not thread-safe
  * with calls in flight on the tree.  No counterpart in the reference, whose
  * kernels have no bounded waits. */
 int hm_set_wait_limit(hm_tree *t, int64_t polls);

@@ -369,6 +369,31 @@ def test_bounded_wait_gives_up_reports_timeout_and_recovers(c1):
         t.set_search_config(sort_bits=-1, join=-1)
 
 
+def test_bucket_join_bounded_wait_reports_timeout_and_recovers(c1):
+    """The TMA-staged bucket join waits for each stage's loads with the same
+    bound: at a limit of 0 every CTA gives up at its first stage, records
+    HM_ETIMEOUT, waits (default bound) for the loads it issued and returns;
+    hm_sync reports the timeout.  With the default limit the join is exact."""
+    keys, sk, t = c1
+    q = dg.gen_point_queries(keys, 1 << 20, 0.5, seed=72)
+    dq = cuda(q)
+    t.set_search_config(join=1)
+    try:
+        out = torch.empty_like(dq)
+        t.set_wait_limit(0)
+        t.search(dq, out)
+        with pytest.raises(HarmoniaError) as e:
+            t.sync()
+        assert e.value.code == -7  # HM_ETIMEOUT
+        t.set_wait_limit(1 << 24)
+        t.search(dq, out)
+        t.sync()
+        assert (out.cpu().numpy() == po.PortTree(sk, dg.values_for(sk)).search(q)).all()
+    finally:
+        t.set_wait_limit(1 << 24)
+        t.set_search_config(join=-1)
+
+
 @pytest.mark.parametrize("smem,levels", [(256, 0), (49152, 2), (200 * 1024, 3)])
 def test_staged_top_levels_budget(smem, levels):
     """2^18 keys: inner levels of 1, 4 and 256 rows; a 256-B budget stages
