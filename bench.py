@@ -219,7 +219,7 @@ def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
     m = 1 << queries_log2
     q = dg.gen_point_queries(keys, m, hit, 2)
 
-    def median_s(fn, reps=3):
+    def median_s(fn, reps=5):
         ts = []
         for _ in range(reps):
             a = time.perf_counter()
@@ -232,7 +232,7 @@ def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
     cpu_out = tree.search(q, threads)
     res = {"build_s": round(build_s, 1), "cores": threads,
            "search": {"value": round(m / sec / 1e6, 3), "unit": UNIT, "ms_per_step": round(sec * 1e3, 1),
-                      "sample": f"the whole {m}-query batch, median of 3"}}
+                      "sample": f"the whole {m}-query batch, median of 5"}}
     if kind == "ppi":
         # the reference's second CPU search: 16 queries per group, AVX2 child
         # search, each next node prefetched (search_cpu_prefetch_NTG_PPI)
@@ -241,13 +241,13 @@ def _cpu_reference_worker(conn, kind, keys_log2, queries_log2, hit):
         same = bool((tree.search_prefetch(q, threads) == cpu_out).all())
         res["search_prefetch"] = {"value": round(m / sec / 1e6, 3), "unit": UNIT, "ms_per_step": round(sec * 1e3, 1),
                                   "same_results": same,
-                                  "sample": f"the whole {m}-query batch, median of 3"}
+                                  "sample": f"the whole {m}-query batch, median of 5"}
         st, ln = dg.gen_ranges(1 << 20, 1, 256, seed=12)
         rec, _ = tree.range_timed(st, ln, threads)
         sec = median_s(lambda: tree.range_timed(st, ln, threads))
         res["range"] = {"value": round(len(st) / sec / 1e6, 3), "unit": "Mranges/s", "ms_per_step": round(sec * 1e3, 1),
                         "records_per_s_m": round(rec / sec / 1e6, 1),
-                        "sample": "2^20 ranges of 1..256 records, the parallel walk of cpu-range.cpp, median of 3"}
+                        "sample": "2^20 ranges of 1..256 records, the parallel walk of cpu-range.cpp, median of 5"}
         if gpu:  # the reference's own GPU search on this GPU, after every GPU leg of the bench
             try:
                 g = po.RefGpuSearch(tree)
