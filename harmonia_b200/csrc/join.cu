@@ -5,7 +5,8 @@
 // contiguous run and the bucket's keys lie in a contiguous range of leaves.
 // Instead of one descent per query (search.cu), a CTA takes a run of one
 // bucket, copies the bucket's leaf records (keys and values, 256 B per
-// 16-key leaf) from HBM into shared memory with 16-B loads in order, and
+// 16-key leaf) from HBM into shared memory in order (2-D tiled TMA loads for
+// 16-key leaves, per-thread cp.async otherwise), and
 // answers every query of the run from shared memory: a binary search over the
 // leaves' first keys (or, for batches of many queries per bucket, a 64-slot
 // directory of them built once per run) picks the leaf, a binary search of
@@ -15,7 +16,9 @@
 // and sequentially, so the DRAM traffic of a batch with more queries than
 // leaves falls from a random 160 B per query to the size of the touched leaf
 // region.  A bucket whose leaves do not fit shared memory (very skewed keys)
-// falls back to a scalar descent per query.
+// falls back to a scalar descent per query.  For batches up to 2^25 queries
+// the results go straight to the queries' positions after the first pre-sort
+// pass (recorded by the second), so only the first pass is undone.
 //
 // The per-query semantics are the reference's (child = number of separators
 // <= key, open-harmonia/src/avx.cpp:2-54; equality in the leaf,

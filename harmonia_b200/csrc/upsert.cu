@@ -9,7 +9,9 @@
 // (rebuild_without_leaf, open-harmonia/src/bpt-ppi-update.cpp:320-463).  The
 // reference never refreshes the GPU copy.
 //
-// Here the epoch runs on the device tree itself:
+// Here the epoch runs on the device tree itself (an epoch of at most 1024
+// keys whose new keys all fit their leaves in one CTA, see small_epoch_kernel;
+// otherwise in these steps):
 //   1. sort the batch by key (stable, payload = input index) and keep the
 //      last occurrence of each key;
 //   2. one thread per key descends; a hit overwrites the value in place
