@@ -7,15 +7,18 @@
 // (open-harmonia/src/buffer.h:88-106).  Here:
 //   * callers submit point-search, range and upsert requests with host
 //     buffers and get a ticket; hm_server_wait blocks (with a timeout) until
-//     the request is done;
+//     the request is done; a point search whose buffers are page-locked (or
+//     device memory) is copied by DMA straight from and to them, the others
+//     through pinned staging filled by helper threads;
 //   * a dispatcher thread admits requests in ticket order while the device
 //     bytes they need fit the budget, coalesces consecutive point searches
 //     (and consecutive ranges) into one launch, and keeps up to `streams`
 //     launches in flight, so requests that arrive while others run on the GPU
 //     are admitted as slots and memory free up (continuous batching);
-//   * an upsert is an epoch barrier: it starts after every earlier request
-//     has finished and before any later one, so each read sees exactly the
-//     upserts submitted before it, the same result it would get alone;
+//   * an upsert is an epoch barrier: it starts after the kernels of every
+//     earlier request have finished (their result copies may still run) and
+//     before any later request, so each read sees exactly the upserts
+//     submitted before it, the same result it would get alone;
 //     consecutive upserts with supplied values are applied as one epoch;
 //   * every wait is bounded: the dispatcher polls launch events and the
 //     caller's wait has a timeout; stop() cancels what has not started.
