@@ -682,7 +682,7 @@ EncodeTiled encoder() {
 // (128-B inner extent, the 128-B swizzle's limit).
 bool leaf_tensor_map(const hm_tree *t, CUtensorMap *m) {
   EncodeTiled enc = encoder();
-  if (!enc || t->cfg.leaf_cap != 16 || t->leaf_index != 0 || t->n_leaf < 1) return false;
+  if (!enc || t->cfg.leaf_cap != 16 || t->leaf_index != 0 || t->n_leaf < 8) return false;  // a box's rows exist
   const cuuint64_t dim[2] = {32, (cuuint64_t)t->n_leaf};
   const cuuint64_t stride[1] = {32 * sizeof(int64_t)};
   const cuuint32_t box[2] = {16, 8};

@@ -294,6 +294,21 @@ def test_bucket_join_matches_oracle(fanout, leaf_cap, nq):
         t.set_search_config(join=-1)
 
 
+@pytest.mark.parametrize("n", [1, 5, 16, 17, 100, 129, 1000, 5000])
+@pytest.mark.parametrize("fanout,leaf_cap", [(64, 16), (128, 64)])
+def test_bucket_join_forced_on_small_trees(n, fanout, leaf_cap):
+    """The join forced on trees of a few leaves (fewer than one 8-record TMA
+    box, a last box reaching past the last leaf): exact against the oracle."""
+    keys = dg.gen_keys(n, seed=500 + n)
+    sk = np.sort(keys)
+    oracle = po.PortTree(sk, dg.values_for(sk))
+    with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys)), fanout=fanout, leaf_cap=leaf_cap) as t:
+        t.set_search_config(join=1)
+        q = dg.gen_point_queries(keys, 5000, 0.6, seed=600 + n)
+        q[:4] = [sk[0], sk[-1], -(2**63), 2**63 - 1]
+        assert (t.search(cuda(q)).cpu().numpy() == oracle.search(q)).all()
+
+
 @pytest.mark.parametrize("ends", [(-(2**62), 2**62), (-(2**63), 2**63 - 2), (2**40, 2**63 - 2)])
 def test_bucket_join_skewed_keys_fall_back(ends):
     # almost all keys in a narrow range: buckets over it hold too many leaves;
