@@ -7,6 +7,6 @@ binding (``native``), the host-side mirror of the reference's tree interface
 loop binding (``serving``).
 """
 from .native import HarmoniaError  # noqa: F401
-from .tree import BPlusTree, launch_count, MAX_KEY, NOT_FOUND  # noqa: F401
+from .tree import BPlusTree, launch_count, trim_memory, MAX_KEY, NOT_FOUND  # noqa: F401
 
-__all__ = ["BPlusTree", "HarmoniaError", "launch_count", "MAX_KEY", "NOT_FOUND"]
+__all__ = ["BPlusTree", "HarmoniaError", "launch_count", "trim_memory", "MAX_KEY", "NOT_FOUND"]

@@ -10,6 +10,8 @@
 #include <mutex>
 #include <set>
 #include <tuple>
+#include <unordered_map>
+#include <vector>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -34,6 +36,121 @@ int cuda_err(cudaError_t e) {
   if (e == cudaErrorMemoryAllocation) return HM_ENOMEM;
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return HM_ENODEVICE;
   return HM_ECUDA;
+}
+
+// ---- device block cache ----
+// Large device blocks (tree arenas, bulk-load and rebuild temporaries,
+// scratch blocks) are kept when their owner releases them and handed to later
+// requests on the same device: a cudaMalloc of a GiB-sized block maps it anew
+// (milliseconds, and variable) and cudaFree synchronises the whole device.
+// A request takes the smallest cached block of at least its size and at most
+// half again as large (plus 64 MiB).  A block is released only once no work
+// is in flight on it (every caller releases after a synchronisation).  At
+// most kCacheCap bytes stay cached (the oldest are freed first);
+// hm_trim_memory frees them all.
+namespace {
+struct CachedBlock {
+  void *p;
+  size_t bytes;
+  int dev;
+};
+std::mutex g_cache_mu;
+std::vector<CachedBlock> g_cache;                           // free blocks, oldest first
+std::unordered_map<void *, std::pair<size_t, int>> g_live;  // blocks handed out by dev_alloc
+size_t g_cached = 0;
+constexpr size_t kCacheCap = (size_t)16 << 30;
+
+void free_block(const CachedBlock &b) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != b.dev) cudaSetDevice(b.dev);
+  cudaFree(b.p);
+  if (cur != b.dev) cudaSetDevice(cur);
+}
+
+// Frees the cached blocks of device dev (-1: every device); returns the bytes freed.
+size_t trim_cache(int dev) {
+  std::vector<CachedBlock> out;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    std::vector<CachedBlock> keep;
+    for (const CachedBlock &b : g_cache) (dev < 0 || b.dev == dev ? out : keep).push_back(b);
+    g_cache.swap(keep);
+    for (const CachedBlock &b : out) g_cached -= b.bytes;
+  }
+  size_t freed = 0;
+  for (const CachedBlock &b : out) {
+    free_block(b);
+    freed += b.bytes;
+  }
+  return freed;
+}
+}  // namespace
+
+cudaError_t dev_alloc(void **p, size_t bytes) {
+  *p = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    int best = -1;
+    for (int i = 0; i < (int)g_cache.size(); i++) {
+      const CachedBlock &b = g_cache[i];
+      if (b.dev == dev && b.bytes >= bytes && b.bytes <= bytes + bytes / 2 + ((size_t)64 << 20) &&
+          (best < 0 || b.bytes < g_cache[best].bytes))
+        best = i;
+    }
+    if (best >= 0) {
+      const CachedBlock b = g_cache[best];
+      g_cache.erase(g_cache.begin() + best);
+      g_cached -= b.bytes;
+      g_live[b.p] = {b.bytes, b.dev};
+      *p = b.p;
+      return cudaSuccess;
+    }
+  }
+  e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation && trim_cache(dev) > 0) {  // cached blocks stand in the way
+    cudaGetLastError();
+    e = cudaMalloc(p, bytes);
+  }
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return e;
+  }
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  g_live[*p] = {bytes, dev};
+  return cudaSuccess;
+}
+
+void dev_release(void *p) {
+  if (!p) return;
+  std::vector<CachedBlock> evict;
+  bool ours = false;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto it = g_live.find(p);
+    if (it != g_live.end()) {
+      ours = true;
+      g_cache.push_back({p, it->second.first, it->second.second});
+      g_cached += it->second.first;
+      g_live.erase(it);
+      while (g_cached > kCacheCap && !g_cache.empty()) {
+        evict.push_back(g_cache.front());
+        g_cached -= g_cache.front().bytes;
+        g_cache.erase(g_cache.begin());
+      }
+    }
+  }
+  if (!ours) cudaFree(p);
+  for (const CachedBlock &b : evict) free_block(b);
+}
+
+void release_after(void *p, cudaStream_t s) {
+  if (!p) return;
+  cudaStreamSynchronize(s);
+  dev_release(p);
 }
 
 // Scratch blocks are plain device allocations that grow by half again when a
@@ -94,7 +211,7 @@ int ScratchLease::acquire(size_t bytes) {
     b.ptr = nullptr;
     b.bytes = 0;
     const size_t want = (size_t)align_up((int64_t)std::max(bytes, bytes / 2 + bytes), 1 << 20);
-    cudaError_t e = cudaMalloc(&b.ptr, want);
+    cudaError_t e = dev_alloc(&b.ptr, want);
     if (e != cudaSuccess) {
       b.ptr = nullptr;
       return cuda_err(e);
@@ -125,11 +242,11 @@ size_t ScratchLease::bytes() const { return idx_ < 0 ? 0 : t_->pool[idx_].bytes;
 
 void free_scratch_pool(hm_tree *t) {
   for (auto &b : t->pool) {
-    if (b.ptr) cudaFree(b.ptr);
+    dev_release(b.ptr);
     if (b.done) cudaEventDestroy(b.done);
   }
   t->pool.clear();
-  for (void *p : t->retired) cudaFree(p);
+  for (void *p : t->retired) dev_release(p);
   t->retired.clear();
 }
 
@@ -273,7 +390,7 @@ cudaStream_t as_stream(hm_stream s) { return reinterpret_cast<cudaStream_t>(s); 
 int free_tree(hm_tree *t) {
   if (!t) return HM_OK;
   cudaDeviceSynchronize();
-  if (t->arena) cudaFree(t->arena);
+  dev_release(t->arena);
   if (t->child_ids) cudaFree(t->child_ids);
   if (t->join_leafb) cudaFree(t->join_leafb);
   if (t->join_leafb_ready) cudaEventDestroy(t->join_leafb_ready);
@@ -531,11 +648,11 @@ int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_c
   size_t tb = align_up(tn * 8, 256);
   size_t temp_bytes = 4 * tb + align_up((int64_t)radix_scratch_bytes(n), 256) + 256;
   char *temp = nullptr;
-  e = cudaMalloc(&t->arena, total);
-  if (e == cudaSuccess) e = cudaMalloc(&temp, temp_bytes);
+  e = dev_alloc(&t->arena, total);
+  if (e == cudaSuccess) e = dev_alloc(reinterpret_cast<void **>(&temp), temp_bytes);
   if (e == cudaSuccess) e = cudaMalloc(&t->d_err, 256);
   if (e != cudaSuccess) {
-    if (temp) cudaFree(temp);
+    dev_release(temp);
     free_tree(t);
     return cuda_err(e);
   }
@@ -562,7 +679,7 @@ int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_c
     e = cudaMemcpyAsync(uk_alt, keys, n * 8, cudaMemcpyDefault, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(vv, vals, n * 8, cudaMemcpyDefault, s);
     if (e != cudaSuccess) {
-      cudaFree(temp);
+      release_after(temp, s);
       free_tree(t);
       return cuda_err(e);
     }
@@ -578,7 +695,7 @@ int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_c
   e = cudaMemcpyAsync(&hflags, flags, 4, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess || hflags) {
-    cudaFree(temp);
+    release_after(temp, s);
     free_tree(t);
     if (e != cudaSuccess) return cuda_err(e);
     return (hflags & 2u) ? HM_EMAXKEY : HM_EDUPLICATE;
@@ -596,7 +713,7 @@ int hm_bulk_load(const int64_t *keys, const int64_t *vals, size_t n_, const hm_c
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = cuda_err(e);
   }
-  cudaFree(temp);
+  release_after(temp, s);
   if (rc) {
     free_tree(t);
     return rc;
@@ -759,6 +876,12 @@ int hm_search(hm_tree *t, const int64_t *q, size_t n_, int64_t *out, hm_stream h
   if (rc) return rc;
   if (e != cudaSuccess) return cuda_err(e);
   return hm_sync(t, hs);
+}
+
+int hm_trim_memory(size_t *released) {
+  const size_t freed = trim_cache(-1);
+  if (released) *released = freed;
+  return HM_OK;
 }
 
 int hm_sync(hm_tree *t, hm_stream hs) {

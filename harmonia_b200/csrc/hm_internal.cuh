@@ -442,6 +442,15 @@ class ScratchLease {
 };
 void free_scratch_pool(hm_tree *t);  // after the device is idle
 
+// Large device blocks through the process's block cache (harmonia.cu):
+// dev_alloc reuses a cached block of the device when one fits, else
+// cudaMalloc; dev_release keeps the block for reuse (no work may still be in
+// flight on it; blocks not from dev_alloc are freed); release_after first
+// waits for stream s.
+cudaError_t dev_alloc(void **p, size_t bytes);
+void dev_release(void *p);
+void release_after(void *p, cudaStream_t s);
+
 // ---- misc ----
 int cuda_err(cudaError_t e);
 

@@ -689,11 +689,11 @@ int rebuild_from_sorted(hm_tree *t, const uint64_t *ck, const int64_t *cv, int64
   int64_t tn = std::max<int64_t>(std::max<int64_t>(n1, nt.n_leaf), 1);
   char *tmp = nullptr;
   void *arena = nullptr;
-  cudaError_t e = cudaMalloc(&arena, total);
-  if (e == cudaSuccess) e = cudaMalloc(&tmp, 2 * al(8 * tn));
+  cudaError_t e = dev_alloc(&arena, total);
+  if (e == cudaSuccess) e = dev_alloc(reinterpret_cast<void **>(&tmp), 2 * al(8 * tn));
   if (e != cudaSuccess) {
-    if (arena) cudaFree(arena);
-    if (tmp) cudaFree(tmp);
+    dev_release(arena);
+    dev_release(tmp);
     return cuda_err(e);
   }
   int64_t *tmp_a = reinterpret_cast<int64_t *>(tmp);
@@ -707,13 +707,14 @@ int rebuild_from_sorted(hm_tree *t, const uint64_t *ck, const int64_t *cv, int64
   nt.leaf_base = reinterpret_cast<int64_t *>(base + off_lbase);
   rc = build_from_sorted(nt, ck, cv, n1, tmp_a, tmp_b, s);
   e = cudaStreamSynchronize(s);
-  cudaFree(tmp);
+  dev_release(tmp);
   if (rc == HM_OK && e != cudaSuccess) rc = cuda_err(e);
   if (rc) {
-    cudaFree(arena);
+    dev_release(arena);
     return rc;
   }
-  cudaFree(t->arena);
+  cudaDeviceSynchronize();  // no call of any stream may still read the old arena
+  dev_release(t->arena);
   t->arena = arena;
   t->arena_bytes = total;
   t->inner = nt.inner;
@@ -903,7 +904,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     const int64_t n0 = t->n_keys, n1 = n0 + nm;
     const int64_t tn = std::max<int64_t>(n1, 1);
     char *tmp = nullptr;
-    e = cudaMalloc(&tmp, 4 * al(8 * tn));
+    e = dev_alloc(reinterpret_cast<void **>(&tmp), 4 * al(8 * tn));
     if (e != cudaSuccess) return cuda_err(e);
     int64_t *ek = reinterpret_cast<int64_t *>(tmp);
     int64_t *ev = reinterpret_cast<int64_t *>(tmp + al(8 * tn));
@@ -914,7 +915,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     merge_rank_kernel<<<grid_for(nm), kThreads, 0, s>>>(mk, mv, nm, ek, n0, true, ck, cv);
     note_launch(2);
     rc = rebuild_from_sorted(t, ck, cv, n1, s);
-    cudaFree(tmp);
+    release_after(tmp, s);
     if (rc) return rc;
   }
   if (t->n_keys == nm || new_ends[0] < t->key_min) t->key_min = new_ends[0];
@@ -1004,7 +1005,7 @@ int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed_
   // a leaf emptied: rebuild from the remaining contents
   const int64_t n1 = t->n_keys, tn = std::max<int64_t>(n1, 1);
   char *tmp = nullptr;
-  e = cudaMalloc(&tmp, 3 * al(8 * tn));
+  e = dev_alloc(reinterpret_cast<void **>(&tmp), 3 * al(8 * tn));
   if (e != cudaSuccess) return cuda_err(e);
   int64_t *ek = reinterpret_cast<int64_t *>(tmp);
   int64_t *ev = reinterpret_cast<int64_t *>(tmp + al(8 * tn));
@@ -1012,7 +1013,7 @@ int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed_
   export_contents(t, ek, ev, s);
   if (n1 > 0) transform_keys_in(ek, ck, n1, s);
   rc = rebuild_from_sorted(t, ck, ev, n1, s);
-  cudaFree(tmp);
+  release_after(tmp, s);
   return rc;
 }
 

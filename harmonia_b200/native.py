@@ -30,7 +30,7 @@ EXPORTS = (
     "hm_search_noalloc", "hm_server_config_default", "hm_server_start", "hm_server_submit",
     "hm_server_wait", "hm_server_get_stats", "hm_server_reset_stats", "hm_server_stop", "hm_server_free",
     "hm_last_cuda_error", "hm_read_keys", "hm_read_ranges", "hm_write_keys", "hm_snapshot_save",
-    "hm_snapshot_load", "hm_delete_batch", "hm_search_baseline",
+    "hm_snapshot_load", "hm_delete_batch", "hm_search_baseline", "hm_trim_memory",
 )
 HM_NOALLOC_MAX_QUERIES = 1 << 20
 
@@ -92,6 +92,7 @@ def lib() -> ctypes.CDLL:
     P, I, SZ = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
     PT = ctypes.POINTER(ctypes.c_void_p)
     L.hm_config_default.argtypes = [ctypes.POINTER(Config)]
+    L.hm_trim_memory.argtypes = [ctypes.POINTER(SZ)]
     L.hm_bulk_load.argtypes = [P, P, SZ, ctypes.POINTER(Config), PT]
     L.hm_search.argtypes = [P, P, SZ, P, P]
     L.hm_search_batches.argtypes = [P, ctypes.POINTER(Batch), I, P]

@@ -375,3 +375,11 @@ class Plan:
 def launch_count() -> int:
     """Kernel launches issued by libharmonia.so in this process."""
     return int(lib().hm_launch_count())
+
+
+def trim_memory() -> int:
+    """Frees the device blocks the library keeps for reuse (arenas,
+    temporaries and scratch of freed trees); returns the bytes freed."""
+    out = ctypes.c_size_t()
+    check(lib().hm_trim_memory(ctypes.byref(out)), "hm_trim_memory")
+    return int(out.value)

@@ -232,6 +232,15 @@ int hm_sync(hm_tree *t, hm_stream s);
 int hm_free(hm_tree *t);
 const char *hm_strerror(int code);
 
+/* Device memory the library keeps for reuse: the arena, build temporaries
+ * and scratch blocks of freed trees and finished rebuilds (up to 16 GiB per
+ * process; a cudaMalloc of a GiB-sized block maps it anew, and cudaFree
+ * synchronises the device).  Later trees and calls on the same device take
+ * blocks from it.  hm_trim_memory frees all of it and reports the bytes in
+ * *released (may be NULL).  No counterpart in the reference, whose
+ * experiments cudaMalloc and cudaFree their buffers per run. */
+int hm_trim_memory(size_t *released);
+
 /* ---- Serving loop ----
  * A request queue in front of one tree.  Callers submit point-search, range
  * and upsert requests with host buffers and wait on the returned ticket.  A

@@ -118,6 +118,26 @@ def test_tiny_batches_on_a_large_tree():
         assert all((a == b).all() for a, b in zip(got, exp))
 
 
+def test_reused_device_blocks_stay_exact():
+    """Trees built after others were freed (and after rebuilds) take their
+    arenas, temporaries and scratch from the library's block cache; their
+    contents and answers stay exact, and hm_trim_memory frees the cache."""
+    from harmonia_b200 import trim_memory
+    keys = dg.gen_keys(1 << 18, seed=131)
+    sk, sv = np.sort(keys), dg.values_for(np.sort(keys))
+    for rep in range(3):
+        with BPlusTree.bulk_load(cuda(keys), cuda(dg.values_for(keys))) as t:  # full leaves
+            bk, bv = dg.gen_upserts(sk, 20000, 0.5, seed=140 + rep)  # overflows: a rebuild
+            t.upsert(cuda(bk), cuda(bv))
+            ek, ev = po.upsert_set(sk, sv, bk, bv)
+            xk, xv = t.export()
+            assert (xk == ek).all() and (xv == ev).all()
+            q = dg.gen_point_queries(ek, 1 << 17, 0.7, seed=150 + rep)
+            assert (t.search(cuda(q)).cpu().numpy() == po.PortTree(ek, ev).search(q)).all()
+    assert trim_memory() > 0
+    assert trim_memory() == 0
+
+
 @pytest.mark.parametrize("fanout,leaf_cap,fill", [(64, 16, 12), (128, 64, 48)])
 def test_small_epochs_one_kernel_path(fanout, leaf_cap, fill):
     """Epochs of at most 1024 keys go through the one-kernel path when every
