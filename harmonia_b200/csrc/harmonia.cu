@@ -153,14 +153,15 @@ void release_after(void *p, cudaStream_t s) {
   dev_release(p);
 }
 
-// Scratch blocks are plain device allocations that grow by half again when a
-// call needs more.  An outgrown block is retired, not freed: cudaFree
-// synchronises the whole device, which would stall reads running on other
-// streams.  Retired blocks are freed with the tree; with growth by half again
-// they add up to at most about twice the largest block.  (A stream-ordered
-// pool that returns memory to the system at every synchronisation, like the
-// device's default pool, maps it anew for each fresh tree: measured 4.6
-// against 2.1 ms for a 4096K-key upsert epoch on a fresh 2^26-key tree.)
+// Scratch blocks come from the block cache above and grow by half again when
+// a call needs more.  An outgrown block is retired, not released: its last
+// use may still run on another stream, and waiting for it would stall that
+// stream's reads.  Retired blocks go back to the cache with the tree (after
+// its device-wide synchronisation); with growth by half again they add up to
+// at most about twice the largest block.  (A stream-ordered pool that returns
+// memory to the system at every synchronisation, like the device's default
+// pool, maps it anew for each fresh tree: measured 4.6 against 2.1 ms for a
+// 4096K-key upsert epoch on a fresh 2^26-key tree.)
 // Idle blocks kept per tree before a busy stream's block is reused instead of
 // adding one (each holds as much as its largest call needed).
 constexpr size_t kPoolBlocks = 8;
@@ -207,7 +208,7 @@ int ScratchLease::acquire(size_t bytes) {
     if (e != cudaSuccess) return cuda_err(e);
   }
   if (b.bytes < bytes) {
-    if (b.ptr) t_->retired.push_back(b.ptr);  // its previous use may still run: freed with the tree
+    if (b.ptr) t_->retired.push_back(b.ptr);  // its previous use may still run: released with the tree
     b.ptr = nullptr;
     b.bytes = 0;
     const size_t want = (size_t)align_up((int64_t)std::max(bytes, bytes / 2 + bytes), 1 << 20);
