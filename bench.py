@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--join", type=int, default=-1, help="1 bucket join, 2 never, -1 auto")
     ap.add_argument("--cpu-sample-log2", type=int, default=22)
     ap.add_argument("--extras", type=int, default=1, help="also time plain / pre-sorted input / e2e")
+    ap.add_argument("--upsert-only", action="store_true",
+                    help="time only the 4096K-key upsert epochs (one JSON line; each timed epoch is an NVTX "
+                         "range named upsert_epoch)")
     return ap.parse_args()
 
 
@@ -466,9 +469,11 @@ def upsert_epochs(keys, dev, steps, peak):
             torch.cuda.synchronize()
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push("upsert_epoch")
             a.record()
             t.upsert(d_bk, d_bv)
             b.record()
+            torch.cuda.nvtx.range_pop()
             torch.cuda.synchronize()
             if i > 0:
                 times.append(a.elapsed_time(b))
@@ -744,7 +749,7 @@ def main():
         return run_reference(args, ws, rank)
     # the reference's CPU trees build in helper processes while the GPU legs
     # run (spawned before any CUDA call)
-    cpu_ref = CpuReference(args) if (rank == 0 and ws == 1 and args.extras) else None
+    cpu_ref = CpuReference(args) if (rank == 0 and ws == 1 and args.extras and not args.upsert_only) else None
 
     import torch
     import torch.distributed as dist
@@ -761,6 +766,12 @@ def main():
     n = 1 << args.keys_log2
     m = 1 << args.queries_log2
     keys = dg.gen_keys(n, 1)
+    if args.upsert_only:
+        peak, kind = peaks()
+        if rank == 0:
+            up = upsert_epochs(keys, dev, args.steps, peak)
+            print(json.dumps({"leg": "upsert", "keys": n, "peak_kind": kind, **up}))
+        return
     vals = dg.values_for(keys)
     q = dg.gen_point_queries(keys, m, args.hit, replicas.query_seed(2, rank))
     d_keys = torch.from_numpy(keys).to(dev)

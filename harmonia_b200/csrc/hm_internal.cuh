@@ -284,6 +284,11 @@ template <typename V>
 bool radix_sort_pairs(uint64_t *ukeys, V *vals, uint64_t *ukeys_alt, V *vals_alt,
                       int64_t n, int begin_bit, int end_bit, void *scratch,
                       cudaStream_t s);
+// The same sort of ukeys with each element's input position (int32, so n <
+// 2^31) as the payload, generated by the first pass; true if the sorted
+// keys and positions ended in the *_alt buffers.
+bool radix_sort_positions(uint64_t *ukeys, int32_t *pos, uint64_t *ukeys_alt, int32_t *pos_alt, int64_t n,
+                          int begin_bit, int end_bit, void *scratch, cudaStream_t s);
 
 // ---- bulk build (build.cu) ----
 int shape(int64_t n, const hm_config &c, int *height, int64_t *lvl_start,

@@ -36,6 +36,7 @@ inline int ctas_for(int64_t n) {
 template <typename K, typename Digit>
 __global__ void __launch_bounds__(kThreads) hist_kernel(const K *__restrict__ keys, int64_t n, int64_t seg,
                                                         Digit dg, int64_t *__restrict__ counts, int nctas) {
+  pdl_enter();
   __shared__ unsigned hist[kWarps][kBins];
   const int w = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&hist[0][0])[i] = 0;
@@ -57,6 +58,7 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const K *__restrict__
                                                            K *__restrict__ keys_out, V *__restrict__ vals_out,
                                                            int64_t n, int64_t seg, Digit dg,
                                                            const int64_t *__restrict__ offsets, int nctas) {
+  pdl_enter();
   __shared__ unsigned wcnt[kWarps][kBins + 1];  // bin kBins collects invalid lanes
   __shared__ unsigned tstart[kBins];
   __shared__ unsigned dcount[kBins];
@@ -164,11 +166,13 @@ void stable_pass(const K *keys, const V *vals, K *keys_out, V *vals_out, int64_t
   const int nctas = ctas_for(n);
   const int64_t seg = (n + nctas - 1) / nctas;
   int64_t *counts = static_cast<int64_t *>(scratch);
-  hist_kernel<K, Digit><<<nctas, kThreads, 0, s>>>(keys, n, seg, dg, counts, nctas);
+  // dependent launches: each kernel waits for its predecessor's results
+  // before touching memory, but is scheduled while that one finishes
+  launch_pdl(hist_kernel<K, Digit>, nctas, kThreads, 0, s, keys, n, seg, dg, counts, nctas);
   note_launch();
   scan_counts(counts, (int64_t)kBins * nctas, s);
-  scatter_kernel<K, V, Digit, GEN_VAL><<<nctas, kThreads, 0, s>>>(keys, vals, keys_out, vals_out, n, seg, dg,
-                                                                   counts, nctas);
+  launch_pdl(scatter_kernel<K, V, Digit, GEN_VAL>, nctas, kThreads, 0, s, keys, vals, keys_out, vals_out, n, seg,
+             dg, static_cast<const int64_t *>(counts), nctas);
   note_launch();
 }
 

@@ -73,6 +73,16 @@ bool radix_sort_pairs(uint64_t *ukeys, V *vals, uint64_t *ukeys_alt, V *vals_alt
   return flipped;
 }
 
+bool radix_sort_positions(uint64_t *ukeys, int32_t *pos, uint64_t *ukeys_alt, int32_t *pos_alt, int64_t n,
+                          int begin_bit, int end_bit, void *scratch, cudaStream_t s) {
+  if (n <= 0 || begin_bit >= end_bit) return false;
+  // the first pass writes each element's input position as its payload
+  radix::stable_pass<uint64_t, int32_t, RadixDigit, true>(ukeys, nullptr, ukeys_alt, pos_alt, n,
+                                                          RadixDigit{begin_bit}, scratch, s);
+  if (begin_bit + 8 >= end_bit) return true;
+  return !radix_sort_pairs<int32_t>(ukeys_alt, pos_alt, ukeys, pos, n, begin_bit + 8, end_bit, scratch, s);
+}
+
 template bool radix_sort_pairs<int64_t>(uint64_t *, int64_t *, uint64_t *, int64_t *, int64_t, int,
                                         int, void *, cudaStream_t);
 template bool radix_sort_pairs<int32_t>(uint64_t *, int32_t *, uint64_t *, int32_t *, int64_t, int,

@@ -45,12 +45,6 @@ unsigned grid_for(int64_t items) {
   return (unsigned)b;
 }
 
-__global__ void iota_kernel(int64_t *p, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = i;
-}
-
 // keep[i] = 1 for the last occurrence of each key in the sorted batch;
 // flags bit1 if a key equals Max_Key.
 __global__ void last_occurrence_kernel(const uint64_t *__restrict__ uk, int64_t n,
@@ -64,7 +58,7 @@ __global__ void last_occurrence_kernel(const uint64_t *__restrict__ uk, int64_t 
   if (f) atomicOr(flags, f);
 }
 
-__global__ void compact_batch_kernel(const uint64_t *__restrict__ uk, const int64_t *__restrict__ idx,
+__global__ void compact_batch_kernel(const uint64_t *__restrict__ uk, const int32_t *__restrict__ idx,
                                      const int64_t *__restrict__ vals, const int32_t *__restrict__ keep,
                                      const int64_t *__restrict__ at, int64_t n,
                                      int64_t *__restrict__ bk, int64_t *__restrict__ bv) {
@@ -79,6 +73,11 @@ __global__ void compact_batch_kernel(const uint64_t *__restrict__ uk, const int6
 }
 
 // Small batches (the serving loop's epochs) skip the multi-pass radix sort:
+// Keys in one upsert or delete epoch, at most: the batch sort carries each
+// key's input position as an int32 (such a batch would need about 200 GB of
+// scratch anyway).
+constexpr int64_t kMaxEpochKeys = 0x7fffffff;
+
 // one CTA sorts (key, input index) pairs in shared memory with a bitonic
 // network, keeps each key's last occurrence and writes the kept keys (and
 // values) in key order to bk/bv and their number to *count; flags bit1 if a
@@ -734,6 +733,7 @@ int rebuild_from_sorted(hm_tree *t, const uint64_t *ck, const int64_t *cv, int64
 int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64_t n, int flags,
                  cudaStream_t s) {
   if (n <= 0) return HM_OK;
+  if (n > kMaxEpochKeys) return HM_ETOOLARGE;
   const int lc = t->cfg.leaf_cap, li = t->leaf_index, f = t->cfg.fanout;
   if (n <= kSmallEpoch && t->n_keys > 0) {  // one kernel, one synchronisation, if every new key fits
     ScratchLease lease(t, s);
@@ -783,8 +783,8 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   auto take4 = [&](void) { char *r = p; p += s4; return r; };
   uint64_t *uk = reinterpret_cast<uint64_t *>(take8());
   uint64_t *uk_alt = reinterpret_cast<uint64_t *>(take8());
-  int64_t *idx = reinterpret_cast<int64_t *>(take8());
-  int64_t *idx_alt = reinterpret_cast<int64_t *>(take8());
+  int32_t *idx = reinterpret_cast<int32_t *>(take8());  // input positions (8-B slots: run_start reuses one)
+  int32_t *idx_alt = reinterpret_cast<int32_t *>(take8());
   int64_t *at = reinterpret_cast<int64_t *>(take8());
   int64_t *bk = reinterpret_cast<int64_t *>(take8());
   int64_t *bv = reinterpret_cast<int64_t *>(take8());
@@ -797,7 +797,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
   int32_t *is_start = reinterpret_cast<int32_t *>(take4());
   int32_t *run_len = reinterpret_cast<int32_t *>(take4());
   int32_t *run_leaf = reinterpret_cast<int32_t *>(take4());
-  int64_t *run_start = idx_alt;  // free once the sort is done
+  int64_t *run_start = nullptr;  // the position buffer the sort leaves free
   void *sort_scratch = p;
   p += al((int64_t)radix_scratch_bytes(n));
   int64_t *lbase_tmp = reinterpret_cast<int64_t *>(p);  // n_leaf + 1 entries
@@ -814,9 +814,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     note_launch();
   } else {
     transform_keys_in(d_keys, uk, n, s);
-    iota_kernel<<<grid_for(n), kThreads, 0, s>>>(idx, n);
-    note_launch();
-    if (radix_sort_pairs<int64_t>(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) {
+    if (radix_sort_positions(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) {
       std::swap(uk, uk_alt);
       std::swap(idx, idx_alt);
     }
@@ -825,7 +823,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
     compact_batch_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, idx, d_vals, keep, at, n, bk, bv);
     note_launch(2);
   }
-  run_start = idx_alt;
+  run_start = reinterpret_cast<int64_t *>(idx_alt);
   int64_t hm_[2] = {0, 0};
   unsigned hf = 0;
   cudaMemcpyAsync(&hm_[0], at + n, 8, cudaMemcpyDeviceToHost, s);
@@ -935,6 +933,7 @@ int upsert_epoch(hm_tree *t, const int64_t *d_keys, const int64_t *d_vals, int64
 int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed_out, cudaStream_t s) {
   if (removed_out) *removed_out = 0;
   if (n <= 0) return HM_OK;
+  if (n > kMaxEpochKeys) return HM_ETOOLARGE;
   const int lc = t->cfg.leaf_cap, li = t->leaf_index, f = t->cfg.fanout;
   const size_t s8 = al(8 * (n + 1)), s4 = al(4 * (n + 1));
   const int64_t scan_n = std::max<int64_t>(n, t->n_leaf) + 1;
@@ -949,8 +948,8 @@ int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed_
   auto take4 = [&](void) { char *r = p; p += s4; return r; };
   uint64_t *uk = reinterpret_cast<uint64_t *>(take8());
   uint64_t *uk_alt = reinterpret_cast<uint64_t *>(take8());
-  int64_t *idx = reinterpret_cast<int64_t *>(take8());
-  int64_t *idx_alt = reinterpret_cast<int64_t *>(take8());
+  int32_t *idx = reinterpret_cast<int32_t *>(take8());
+  int32_t *idx_alt = reinterpret_cast<int32_t *>(take8());
   int64_t *at = reinterpret_cast<int64_t *>(take8());
   int64_t *bk = reinterpret_cast<int64_t *>(take8());
   int32_t *keep = reinterpret_cast<int32_t *>(take4());
@@ -970,9 +969,7 @@ int delete_epoch(hm_tree *t, const int64_t *d_keys, int64_t n, int64_t *removed_
     note_launch();
   } else {
     transform_keys_in(d_keys, uk, n, s);
-    iota_kernel<<<grid_for(n), kThreads, 0, s>>>(idx, n);
-    note_launch();
-    if (radix_sort_pairs<int64_t>(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) std::swap(uk, uk_alt);
+    if (radix_sort_positions(uk, idx, uk_alt, idx_alt, n, 0, 64, sort_scratch, s)) std::swap(uk, uk_alt);
     last_occurrence_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, n, keep, dflags);
     exclusive_scan_i32(keep, at, n, scan_scratch, s);
     compact_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(uk, keep, at, n, bk);

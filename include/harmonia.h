@@ -25,8 +25,9 @@
  * host threads on any streams, and their work may overlap on the device: each
  * call leases a scratch block of its own from the tree's pool, ordered on the
  * device after that block's previous use; a block that is too small is
- * replaced by one half again as large and the old one is freed only with the
- * tree, so no call frees device memory (which would synchronise the device).
+ * replaced by one half again as large and the old one is released only with
+ * the tree, so no call frees device memory (which would synchronise the
+ * device).
  * Host-buffer searches of one tree take turns (they share the tree's copy
  * streams and pinned staging).  Calls that change the tree or its settings
  * (hm_upsert_batch, hm_delete_batch, hm_set_search_config, hm_autotune,
@@ -188,6 +189,7 @@ int hm_range_between(hm_tree *t, const int64_t *start, const int64_t *end, size_
 /* Applies one epoch of upserts on the GPU: existing keys are updated in
  * place, new keys are merged into their leaves, and leaves that overflow
  * trigger a rebuild.  Within one batch the last occurrence of a key wins.
+ * At most 2^31 - 1 keys per batch (HM_ETOOLARGE beyond).
  * Replaces: BPlusTree::insert_parallel_Newupdate_batch and its worker
  * (open-harmonia/src/bpt-ppi-update-batch.cpp:10-200), insert_Newupdate and
  * rebuild_without_leaf (open-harmonia/src/bpt-ppi-update.cpp:99-138,320-463). */
@@ -394,6 +396,7 @@ int hm_write_keys(const char *path, const int64_t *keys, size_t n);
 
 /* One epoch of deletes: every listed key that is stored is removed (absent
  * keys and repeats are ignored); *removed (may be NULL) receives the count.
+ * At most 2^31 - 1 keys per batch (HM_ETOOLARGE beyond).
  * Searches and range scans afterwards see the remaining keys only, and a later
  * upsert can store a removed key again.  Keys may be host or device memory;
  * returns when done.  No counterpart in the reference, whose
