@@ -1047,6 +1047,7 @@ int hm_range_between(hm_tree *t, const int64_t *start, const int64_t *end, size_
 int hm_delete_batch(hm_tree *t, const int64_t *keys, size_t n_, size_t *removed, hm_stream hs) {
   if (removed) *removed = 0;
   if (!t || (n_ > 0 && !keys)) return HM_EINVAL;
+  if (n_ > (size_t)0x7fffffff) return HM_ETOOLARGE;  // before anything is copied
   const int64_t n = (int64_t)n_;
   if (n == 0) return HM_OK;
   cudaStream_t s = as_stream(hs);
@@ -1075,6 +1076,7 @@ int hm_upsert_batch(hm_tree *t, const int64_t *keys, const int64_t *vals, size_t
                     hm_stream hs) {
   if (!t || (n_ > 0 && (!keys || !vals))) return HM_EINVAL;
   if (flags != HM_UPSERT_SUPPLIED && flags != HM_UPSERT_REF_KEY_MINUS_1) return HM_EINVAL;
+  if (n_ > (size_t)0x7fffffff) return HM_ETOOLARGE;  // before anything is copied
   const int64_t n = (int64_t)n_;
   if (n == 0) return HM_OK;
   cudaStream_t s = as_stream(hs);

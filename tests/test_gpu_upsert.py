@@ -88,6 +88,24 @@ def test_upsert_into_empty_tree_and_errors():
         assert t.export()[0].tolist() == [-3, 5, 100]
 
 
+def test_oversized_batches_are_rejected_before_any_copy():
+    """Upsert and delete batches hold at most 2^31 - 1 keys (the batch sort
+    carries 32-bit input positions): a larger count gets HM_ETOOLARGE at the
+    entry point, before a byte of the (here one-element) buffers is read, and
+    the tree is unchanged."""
+    import ctypes
+    from harmonia_b200.native import lib
+    with BPlusTree.bulk_load(np.array([1, 2, 3], np.int64), np.array([10, 20, 30], np.int64)) as t:
+        one = torch.zeros(1, dtype=torch.int64, device="cuda")
+        p = ctypes.c_void_p(one.data_ptr())
+        assert lib().hm_upsert_batch(t._h, p, p, 1 << 31, 0, None) == -11
+        removed = ctypes.c_size_t(7)
+        assert lib().hm_delete_batch(t._h, p, 1 << 31, ctypes.byref(removed), None) == -11
+        assert removed.value == 0
+        k, v = t.export()
+        assert k.tolist() == [1, 2, 3] and v.tolist() == [10, 20, 30]
+
+
 def test_many_small_epochs_stay_exact():
     keys = dg.gen_keys(1 << 14, seed=41)
     sk, sv = np.sort(keys), dg.values_for(np.sort(keys))
