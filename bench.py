@@ -768,9 +768,12 @@ def main():
     keys = dg.gen_keys(n, 1)
     if args.upsert_only:
         peak, kind = peaks()
-        if rank == 0:
+        if rank == 0:  # one GPU's epochs; other ranks only wait
             up = upsert_epochs(keys, dev, args.steps, peak)
             print(json.dumps({"leg": "upsert", "keys": n, "peak_kind": kind, **up}))
+        if ws > 1:
+            dist.barrier()
+            dist.destroy_process_group()
         return
     vals = dg.values_for(keys)
     q = dg.gen_point_queries(keys, m, args.hit, replicas.query_seed(2, rank))
