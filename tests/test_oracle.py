@@ -88,6 +88,52 @@ def test_reference_rule_upsert_equals_supplied_key_minus_1(c1):
     assert (a[0] == b[0]).all() and (a[1] == b[1]).all()
 
 
+# One case of the direct upsert comparison, run in a child process: the
+# reference ends its process (exit code 0) when an update would split the
+# root (open-harmonia/src/bpt.cpp:336-339), which must fail the test rather
+# than end the test run.
+_UPSERT_CASE = """
+import sys, numpy as np
+sys.path.insert(0, sys.argv[4])
+from harmonia_b200 import datagen as dg
+from oracle import pyoracle as po
+n, frac, seed = int(sys.argv[1]), float(sys.argv[2]), int(sys.argv[3])
+keys = dg.gen_keys(n, seed)
+cur_k = np.sort(keys)
+cur_v = dg.values_for(cur_k)
+ref = po.RefTree(keys, dg.values_for(keys))
+for e in range(2):
+    bk, bv = dg.gen_upserts(cur_k, max(1, n // 8), frac, seed * 10 + e)
+    ref.upsert(bk, bv)
+    cur_k, cur_v = po.upsert_set(cur_k, cur_v, bk, bv, ref_rule=True)
+    rk, rv = ref.export()
+    assert len(rk) == len(cur_k) and (rk == cur_k).all() and (rv == cur_v).all(), ("contents", e)
+    q = dg.gen_point_queries(cur_k, 4096, 0.5, seed + e)
+    assert (ref.search(q) == po.PortTree(cur_k, cur_v).search(q)).all(), ("search", e)
+print("CASE-OK", len(cur_k))
+"""
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference library not built in this checkout")
+@pytest.mark.parametrize("frac", [0.0, 0.05, 0.5, 1.0])
+@pytest.mark.parametrize("n", [5000, 1 << 16, 1 << 18])
+def test_upsert_restatement_matches_reference_batched_update(n, frac):
+    """The restatement of an upsert epoch (po.upsert_set under the reference's
+    rule, the oracle of every GPU upsert test) against the reference's own
+    BPlusTree::insert_parallel_Newupdate_batch
+    (open-harmonia/src/bpt-ppi-update-batch.cpp:86-200): two epochs of n/8
+    keys in a row, from no new keys to all new, the sorted contents equal
+    after each, and searches through the reference's post-update descent
+    equal the restatement's on the new contents."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _UPSERT_CASE, str(n), str(frac), "7", root],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "CASE-OK" in r.stdout, (r.returncode, r.stdout[-500:], r.stderr[-2000:])
+
+
 def test_upsert_last_occurrence_wins():
     sk = np.array([10, 20, 30], np.int64)
     sv = np.array([1, 2, 3], np.int64)
